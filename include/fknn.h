@@ -1,0 +1,150 @@
+/*
+ * fknn.h -- C ABI of the B200 filtered k-nearest-neighbour engine.
+ *
+ * Plain pointers and sizes only.  Every entry point returns an int status
+ * (FKNN_OK or a negative FKNN_E* code) and never aborts the process; the
+ * text of the last failure on the calling thread is in fknn_last_error().
+ *
+ * Pointers passed to fknn_search / fknn_sq8_* may be host memory (pageable
+ * or pinned) or device memory on the index's device; the library tells them
+ * apart with cudaPointerGetAttributes and copies as needed.
+ *
+ * Reference interfaces replaced (paths inside KevinZeng08/sigmod-2024-contest):
+ *   fknn_bruteforce_rows   <- Bruteforce(nodes, queries, gt)          utils.h:80
+ *   fknn_index_create +
+ *   fknn_search(EXACT)     <- the same exact filtered top-k, resident  utils.h:80-158
+ *   fknn_search(BF16/FP8)  <- HybridGraph::BatchSearch's brute-force
+ *                             + FP32 re-rank leg                       hybrid_graph.cpp:201-229
+ *   fknn_sq8_bruteforce    <- bruteforce(dim, k, ...)                  bruteforce.h:244
+ *   fknn_sq8_bruteforce_subgraph <- bruteforce_subgraph(...)           bruteforce.h:267
+ *   fknn_sq8_sym_train     <- SQ8SymmetricQuantizer::train/encode      pyglass/glass/quant/sq8_sym_quant.hpp:32-74
+ */
+#ifndef FKNN_H_
+#define FKNN_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FKNN_OK 0
+#define FKNN_EINVAL (-1)      /* bad argument: shape, query type, non-finite value, k */
+#define FKNN_ENOMEM (-2)      /* device or host allocation failed, or over the HBM budget */
+#define FKNN_ECUDA (-3)       /* a CUDA runtime call failed */
+#define FKNN_ETIMEOUT (-4)    /* a bounded device wait gave up */
+#define FKNN_EUNSUPPORTED (-5) /* mode not built into this index */
+#define FKNN_ENODEV (-6)      /* no CUDA device */
+
+/* Search modes. */
+#define FKNN_MODE_EXACT_FP32 0 /* ids bit-identical to utils.h:80 Bruteforce */
+#define FKNN_MODE_BF16_RERANK 1 /* BF16 tensor-core screen, FP32 re-rank, FP64 boundary fix-up */
+#define FKNN_MODE_FP8_RERANK 2  /* FP8-e4m3 per-dimension-scaled screen, same re-rank */
+
+#define FKNN_DIM 100 /* the contest's vector width (utils.h:255 vec_dim) */
+
+typedef struct fknn_index fknn_index;
+
+typedef struct fknn_index_opts {
+  int device;           /* CUDA device ordinal */
+  int build_bf16;       /* keep BF16 copies for FKNN_MODE_BF16_RERANK */
+  int build_fp8;        /* keep FP8-e4m3 per-dim codes for FKNN_MODE_FP8_RERANK */
+  uint64_t hbm_budget;  /* bytes the index may hold on the device; 0 = no limit */
+} fknn_index_opts;
+
+typedef struct fknn_search_opts {
+  int mode;             /* FKNN_MODE_* */
+  uint32_t kprime;      /* candidate width for the reduced-precision modes (0 = default 400) */
+} fknn_search_opts;
+
+/* Per-call statistics (optional out-parameter of fknn_search_ex). */
+typedef struct fknn_search_stats {
+  uint64_t pairs_screened;     /* (query, row) pairs the screening contraction evaluated, masked ones included */
+  uint64_t pairs_passing;      /* pairs that pass the predicate (sum of slab sizes), all queries */
+  uint64_t pairs_contraction;  /* passing pairs of the queries the contraction served */
+  uint32_t n_tiles;            /* query tiles of the contraction */
+  uint32_t n_work_items;       /* (tile, row chunk) work items */
+  uint32_t n_small;            /* queries routed to the row-by-row exact scan */
+  uint32_t n_overflow;         /* queries re-run by the exact scan after a candidate overflow */
+  uint32_t n_boundary_f64;     /* candidates recomputed in FP64 at the k-th boundary */
+  uint32_t kernel_launches;    /* kernels this call launched */
+  float ms_plan;               /* host planning time */
+  float ms_screen;             /* device time of the screening contraction (CUDA events, launching stream) */
+  float ms_merge;              /* device time of the merge + exact re-score */
+  float ms_scan;               /* device time of the row-by-row exact scans */
+} fknn_search_stats;
+
+/* Library version (major*10000 + minor*100 + patch). */
+int fknn_version(void);
+
+/* Text of the last failure on this thread ("" if none). */
+const char *fknn_last_error(void);
+
+/* Builds a resident index on opts->device from SoA columns in host memory:
+ * vecs n x dim float32 (dim must be 100), labels n float32 (category, read
+ * as int32 like utils.h:109), ts n float32 (timestamp).  Values must be
+ * finite; |label| < 2^31; |vec| <= 1e15.  Rows keep their position as id. */
+int fknn_index_create(const float *vecs, const float *labels, const float *ts, uint64_t n,
+                      uint32_t dim, const fknn_index_opts *opts, fknn_index **out);
+
+int fknn_index_destroy(fknn_index *index);
+
+/* Device bytes held by the index. */
+int fknn_index_bytes(const fknn_index *index, uint64_t *bytes);
+
+/* Filtered top-k for nq queries.
+ *   qvecs : nq x 100 float32
+ *   metas : nq x 4 float32 (type, v, l, r) -- the contest query header
+ *           (utils.h:98-101); type 0 none, 1 label==v, 2 l<=ts<=r, 3 both.
+ *   ids   : nq x k uint32, ascending (distance, id); UINT32_MAX padding
+ *           when fewer than k rows pass.
+ *   dists : nq x k float32 or NULL; +inf padding.
+ *   stream: cudaStream_t or NULL (the legacy default stream).
+ * Returns when the results are in ids/dists (host or device). */
+int fknn_search(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,
+                int mode, uint32_t *ids, float *dists, void *stream);
+
+/* As fknn_search with options and statistics (stats may be NULL). */
+int fknn_search_ex(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,
+                   const fknn_search_opts *opts, uint32_t *ids, float *dists, void *stream,
+                   fknn_search_stats *stats);
+
+/* Number of rows passing each query's predicate (the selectivity numerator of
+ * hybrid_graph.cpp:168-200), from the index's sorted attribute columns. */
+int fknn_count_matches(fknn_index *index, const float *metas, uint32_t nq, uint32_t *counts, void *stream);
+
+/* Predicate evaluation + row compaction over the attribute columns for ONE
+ * predicate (type, v, l, r): writes the ids of passing rows in increasing
+ * order into out_ids (capacity n) and their number into *count. */
+int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, uint64_t *count, void *stream);
+
+/* Drop-in for utils.h:80 Bruteforce on contest-layout rows: nodes n x 102
+ * (label, ts, 100 dims), queries nq x 104 (type, v, l, r, 100 dims), gt
+ * nq x 100 ascending (distance, id).  Builds a temporary index on device 0. */
+int fknn_bruteforce_rows(const float *nodes, uint32_t n, const float *queries, uint32_t nq, uint32_t *gt);
+
+/* Symmetric SQ8 (sq8_sym_quant.hpp:32-74): alpha = max|x| over n x 100
+ * vectors; codes n x 112 int8 = round(clamp(x/alpha,-1,1)*127), zero-padded. */
+int fknn_sq8_sym_train(const float *vecs, uint64_t n, float *alpha, int8_t *codes);
+/* Encodes with a given alpha (sq8_sym_quant.hpp:63-74). */
+int fknn_sq8_sym_encode(const float *vecs, uint64_t n, float alpha, int8_t *codes);
+
+/* Drop-in for bruteforce (bruteforce.h:244).  Same arguments; codes_in is a
+ * slab of npoints x 112 int8 codes, queries_in nqueries x 112 int8.  Unlike
+ * the reference, nqueries is honoured: closest_points is nqueries x k, each
+ * row in the reference's heap-array order.  dim and alpha are ignored, as in
+ * the reference.  Requires 1 <= k <= npoints. */
+int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoints, const char *codes_in,
+                        float alpha, size_t nqueries, const int8_t *queries_in);
+
+/* Drop-in for bruteforce_subgraph (bruteforce.h:267): also writes
+ * distances[k] = heap distance * alpha * alpha. */
+int fknn_sq8_bruteforce_subgraph(size_t dim, size_t k, int *closest_points, float *distances, size_t npoints,
+                                 const char *codes_in, float alpha, size_t nqueries, const int8_t *queries_in);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FKNN_H_ */

@@ -1,0 +1,146 @@
+"""ctypes loader of the CPU checker.  TEST INFRASTRUCTURE ONLY.
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use this
+module, and only as the checker / the timed CPU baseline; the product
+library never calls it.
+
+  restatement : oracle/libfknn_oracle.so  (oracle/fknn_oracle.c)
+  reference   : oracle/_ref/libref_exact.so, oracle/_ref/libref_sq8.so, the
+                reference's own code compiled from its sources (oracle/Makefile)
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from ctypes import POINTER, c_double, c_float, c_int, c_int8, c_uint32, c_uint64, c_void_p
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ORACLE_SO = os.path.join(HERE, "libfknn_oracle.so")
+REF_EXACT_SO = os.path.join(HERE, "_ref", "libref_exact.so")
+REF_SQ8_SO = os.path.join(HERE, "_ref", "libref_sq8.so")
+DIM = 100
+
+_o = None
+_re = None
+_rs = None
+
+
+def build(ref: bool = False) -> None:
+    """make -C oracle (and the reference objects when the sources are present)."""
+    targets = ["all"] + (["ref"] if ref else [])
+    subprocess.run(["make", "-s", "-C", HERE] + targets, check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _o
+    if _o is None:
+        if not os.path.exists(ORACLE_SO):
+            build()
+        L = ctypes.CDLL(ORACLE_SO)
+        L.oracle_normal_l2.restype = c_float
+        L.oracle_normal_l2.argtypes = [c_void_p, c_void_p, c_uint32]
+        L.oracle_exact_knn.restype = c_int
+        L.oracle_exact_knn.argtypes = [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_uint32,
+                                       c_uint32, c_void_p, c_void_p, c_int]
+        L.oracle_exact_knn_f64.restype = c_int
+        L.oracle_exact_knn_f64.argtypes = L.oracle_exact_knn.argtypes
+        L.oracle_count_matches.restype = None
+        L.oracle_count_matches.argtypes = [c_void_p, c_void_p, c_uint32, c_void_p, c_uint32, c_void_p]
+        L.oracle_sq8_sym_alpha.restype = c_float
+        L.oracle_sq8_sym_alpha.argtypes = [c_void_p, c_uint64]
+        L.oracle_sq8_sym_encode.restype = None
+        L.oracle_sq8_sym_encode.argtypes = [c_void_p, c_uint64, c_float, c_void_p]
+        L.oracle_l2sqr_sq8_sym.restype = ctypes.c_int32
+        L.oracle_l2sqr_sq8_sym.argtypes = [c_void_p, c_void_p]
+        L.oracle_sq8_bruteforce.restype = c_int
+        L.oracle_sq8_bruteforce.argtypes = [c_uint64, c_void_p, c_void_p, c_uint64, c_void_p, c_float, c_void_p]
+        _o = L
+    return _o
+
+
+def ref_exact() -> ctypes.CDLL | None:
+    """The reference Bruteforce (utils.h:80) compiled from its sources, or None."""
+    global _re
+    if _re is None and os.path.exists(REF_EXACT_SO):
+        L = ctypes.CDLL(REF_EXACT_SO)
+        L.ref_exact_bruteforce.restype = c_int
+        L.ref_exact_bruteforce.argtypes = [c_void_p, c_uint32, c_void_p, c_uint32, c_void_p, POINTER(c_double)]
+        L.ref_normal_l2.restype = c_float
+        L.ref_normal_l2.argtypes = [c_void_p, c_void_p, c_uint32]
+        _re = L
+    return _re
+
+
+def ref_sq8() -> ctypes.CDLL | None:
+    global _rs
+    if _rs is None and os.path.exists(REF_SQ8_SO):
+        L = ctypes.CDLL(REF_SQ8_SO)
+        L.ref_l2sqr_sq8_sym.restype = c_int
+        L.ref_l2sqr_sq8_sym.argtypes = [c_void_p, c_void_p]
+        L.ref_sq8_sym_train.restype = None
+        L.ref_sq8_sym_train.argtypes = [c_void_p, c_uint32, POINTER(c_float), c_void_p]
+        L.ref_sq8_sym_encode.restype = None
+        L.ref_sq8_sym_encode.argtypes = [c_void_p, c_float, c_void_p]
+        L.ref_sq8_bruteforce.restype = None
+        L.ref_sq8_bruteforce.argtypes = [c_uint64, c_void_p, c_uint64, c_void_p, c_float, c_void_p]
+        L.ref_sq8_bruteforce_subgraph.restype = None
+        L.ref_sq8_bruteforce_subgraph.argtypes = [c_uint64, c_void_p, c_void_p, c_uint64, c_void_p, c_float, c_void_p]
+        _rs = L
+    return _rs
+
+
+def _c(a, dt):
+    return np.ascontiguousarray(a, dtype=dt)
+
+
+def exact_knn(vecs, labels, ts, qvecs, metas, k: int = 100, nthreads: int = 0, f64: bool = False):
+    """Restated utils.h:80 over SoA columns -> (ids (nq,k) u32, dists (nq,k))."""
+    vecs, labels, ts = _c(vecs, np.float32), _c(labels, np.float32), _c(ts, np.float32)
+    qvecs, metas = _c(qvecs, np.float32), _c(metas, np.float32)
+    nq = qvecs.shape[0]
+    ids = np.empty((nq, k), dtype=np.uint32)
+    dists = np.empty((nq, k), dtype=np.float64 if f64 else np.float32)
+    nthreads = nthreads or os.cpu_count() or 1
+    fn = lib().oracle_exact_knn_f64 if f64 else lib().oracle_exact_knn
+    rc = fn(vecs.ctypes.data, labels.ctypes.data, ts.ctypes.data, vecs.shape[0], qvecs.ctypes.data,
+            metas.ctypes.data, nq, k, ids.ctypes.data, dists.ctypes.data, nthreads)
+    if rc != 0:
+        raise ValueError(f"oracle_exact_knn failed ({rc})")
+    return ids, dists
+
+
+def count_matches(labels, ts, metas) -> np.ndarray:
+    labels, ts, metas = _c(labels, np.float32), _c(ts, np.float32), _c(metas, np.float32)
+    out = np.empty(metas.shape[0], dtype=np.uint32)
+    lib().oracle_count_matches(labels.ctypes.data, ts.ctypes.data, labels.shape[0], metas.ctypes.data,
+                               metas.shape[0], out.ctypes.data)
+    return out
+
+
+def sq8_sym_train(vecs):
+    vecs = _c(vecs, np.float32)
+    a = lib().oracle_sq8_sym_alpha(vecs.ctypes.data, vecs.size)
+    codes = np.empty((vecs.shape[0], 112), dtype=np.int8)
+    lib().oracle_sq8_sym_encode(vecs.ctypes.data, vecs.shape[0], c_float(a), codes.ctypes.data)
+    return a, codes
+
+
+def sq8_sym_encode(vecs, alpha):
+    vecs = _c(vecs, np.float32).reshape(-1, DIM)
+    codes = np.empty((vecs.shape[0], 112), dtype=np.int8)
+    lib().oracle_sq8_sym_encode(vecs.ctypes.data, vecs.shape[0], c_float(alpha), codes.ctypes.data)
+    return codes
+
+
+def sq8_bruteforce(k, codes, alpha, query, with_dists=False):
+    codes, query = _c(codes, np.int8), _c(query, np.int8)
+    ids = np.empty(k, dtype=np.int32)
+    d = np.empty(k, dtype=np.float32) if with_dists else None
+    rc = lib().oracle_sq8_bruteforce(k, ids.ctypes.data, d.ctypes.data if with_dists else None, codes.shape[0],
+                                     codes.ctypes.data, c_float(alpha), query.ctypes.data)
+    if rc != 0:
+        raise ValueError("oracle_sq8_bruteforce: need 1 <= k <= npoints")
+    return (ids, d) if with_dists else ids

@@ -1,0 +1,349 @@
+// C ABI entry points (include/fknn.h), error plumbing and device memory.
+#include <cstdio>
+#include <cstring>
+#include <new>
+
+#include "fknn_internal.cuh"
+
+namespace fknn {
+
+thread_local uint32_t g_launches = 0;
+static thread_local std::string g_err;
+
+void set_error(const std::string &msg) { g_err = msg; }
+
+int cuda_fail(cudaError_t e, const char *what) {
+  g_err = std::string("CUDA error ") + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ") in " + what;
+  if (e == cudaErrorMemoryAllocation) return FKNN_ENOMEM;
+  if (e == cudaErrorNoDevice || e == cudaErrorInsufficientDriver) return FKNN_ENODEV;
+  return FKNN_ECUDA;
+}
+
+int dev_alloc(fknn_index *idx, void **p, size_t bytes) {
+  if (idx->hbm_budget && idx->bytes + bytes > idx->hbm_budget) {
+    set_error("device allocation of " + std::to_string(bytes) + " bytes exceeds the index HBM budget of " +
+              std::to_string(idx->hbm_budget));
+    return FKNN_ENOMEM;
+  }
+  cudaError_t e = cudaMalloc(p, bytes ? bytes : 16);
+  if (e != cudaSuccess) {
+    *p = nullptr;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  idx->bytes += bytes;
+  return FKNN_OK;
+}
+
+static void dev_free(fknn_index *idx, void *p, size_t bytes) {
+  if (p) {
+    cudaFree(p);
+    idx->bytes -= bytes;
+  }
+}
+
+int ws_get(fknn_index *idx, int slot, size_t bytes, void **p) {
+  DevBuf &b = idx->ws[slot];
+  if (b.bytes < bytes) {
+    // in-flight work may still read the old buffer
+    cudaDeviceSynchronize();
+    dev_free(idx, b.p, b.bytes);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 4;
+    int rc = dev_alloc(idx, &b.p, want);
+    if (rc) return rc;
+    b.bytes = want;
+  }
+  *p = b.p;
+  return FKNN_OK;
+}
+
+int hs_get(fknn_index *idx, int slot, size_t bytes, void **p) {
+  HostBuf &b = idx->hs[slot];
+  if (b.bytes < bytes) {
+    cudaDeviceSynchronize();
+    if (b.p) cudaFreeHost(b.p);
+    b.p = nullptr;
+    b.bytes = 0;
+    size_t want = bytes + bytes / 4 + 64;
+    cudaError_t e = cudaMallocHost(&b.p, want);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaMallocHost");
+    b.bytes = want;
+  }
+  *p = b.p;
+  return FKNN_OK;
+}
+
+static bool is_device_ptr(const void *p) {
+  if (!p) return false;
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+static void free_index(fknn_index *idx) {
+  if (!idx) return;
+  cudaSetDevice(idx->device);
+  cudaDeviceSynchronize();
+  cudaFree(idx->vecs);
+  cudaFree(idx->norms);
+  cudaFree(idx->labels_f);
+  cudaFree(idx->ts_f);
+  for (int o = 0; o < 2; ++o) {
+    cudaFree(idx->ord[o].blocks);
+    cudaFree(idx->ord[o].perm);
+    cudaFree(idx->ord[o].ts);
+    cudaFree(idx->ord[o].label);
+    cudaFree(idx->bf16_blocks[o]);
+    cudaFree(idx->fp8_blocks[o]);
+  }
+  cudaFree(idx->fp8_scale);
+  for (auto &b : idx->ws) cudaFree(b.p);
+  for (auto &b : idx->hs)
+    if (b.p) cudaFreeHost(b.p);
+  cudaFree(idx->d_flag);
+  if (idx->own_stream) cudaStreamDestroy(idx->own_stream);
+  delete idx;
+}
+
+}  // namespace fknn
+
+using namespace fknn;
+
+extern "C" {
+
+int fknn_version(void) { return 100; }
+
+const char *fknn_last_error(void) { return g_err.c_str(); }
+
+int fknn_index_create(const float *vecs, const float *labels, const float *ts, uint64_t n, uint32_t dim,
+                      const fknn_index_opts *opts, fknn_index **out) {
+  g_err.clear();
+  g_launches = 0;
+  if (!out) {
+    set_error("fknn_index_create: out is NULL");
+    return FKNN_EINVAL;
+  }
+  *out = nullptr;
+  if (dim != (uint32_t)DIM) {
+    set_error("fknn_index_create: dim must be 100");
+    return FKNN_EINVAL;
+  }
+  if (n == 0 || n >= (1ull << 31)) {
+    set_error("fknn_index_create: n must be in [1, 2^31)");
+    return FKNN_EINVAL;
+  }
+  if (!vecs || !labels || !ts) {
+    set_error("fknn_index_create: NULL input column");
+    return FKNN_EINVAL;
+  }
+  int ndev = 0;
+  cudaError_t e = cudaGetDeviceCount(&ndev);
+  if (e != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    set_error("fknn_index_create: no CUDA device");
+    return FKNN_ENODEV;
+  }
+  fknn_index *idx = new (std::nothrow) fknn_index();
+  if (!idx) return FKNN_ENOMEM;
+  idx->device = opts ? opts->device : 0;
+  idx->hbm_budget = opts ? opts->hbm_budget : 0;
+  idx->n = n;
+  if (idx->device < 0 || idx->device >= ndev) {
+    delete idx;
+    set_error("fknn_index_create: bad device ordinal");
+    return FKNN_EINVAL;
+  }
+  int rc = FKNN_OK;
+  e = cudaSetDevice(idx->device);
+  if (e != cudaSuccess) rc = cuda_fail(e, "cudaSetDevice");
+  if (!rc) {
+    e = cudaStreamCreateWithFlags(&idx->own_stream, cudaStreamNonBlocking);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate");
+  }
+  if (!rc) {
+    e = cudaMalloc(&idx->d_flag, 64);
+    if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc");
+  }
+  if (!rc) rc = build_index(idx, vecs, labels, ts, idx->own_stream);
+  if (!rc && opts && (opts->build_bf16 || opts->build_fp8)) {
+    set_error("fknn_index_create: reduced-precision copies are not available in this build");
+    rc = FKNN_EUNSUPPORTED;
+  }
+  // build temporaries are not needed by searches
+  for (int s = 10; s < 16; ++s) {
+    if (idx->ws[s].p) {
+      cudaFree(idx->ws[s].p);
+      idx->bytes -= idx->ws[s].bytes;
+      idx->ws[s].p = nullptr;
+      idx->ws[s].bytes = 0;
+    }
+  }
+  if (rc) {
+    free_index(idx);
+    return rc;
+  }
+  *out = idx;
+  return FKNN_OK;
+}
+
+int fknn_index_destroy(fknn_index *index) {
+  free_index(index);
+  return FKNN_OK;
+}
+
+int fknn_index_bytes(const fknn_index *index, uint64_t *bytes) {
+  if (!index || !bytes) return FKNN_EINVAL;
+  *bytes = index->bytes;
+  return FKNN_OK;
+}
+
+int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,
+                   const fknn_search_opts *opts, uint32_t *ids, float *dists, void *stream, fknn_search_stats *stats) {
+  g_err.clear();
+  g_launches = 0;
+  if (stats) std::memset(stats, 0, sizeof(*stats));
+  if (!idx) {
+    set_error("fknn_search: NULL index");
+    return FKNN_EINVAL;
+  }
+  const int mode = opts ? opts->mode : FKNN_MODE_EXACT_FP32;
+  if (k == 0 || k > (uint32_t)KMAX_TILE) {
+    set_error("fknn_search: k must be in [1, 128]");
+    return FKNN_EINVAL;
+  }
+  if (nq == 0) return FKNN_OK;
+  if (!qvecs || !metas || !ids) {
+    set_error("fknn_search: NULL qvecs/metas/ids");
+    return FKNN_EINVAL;
+  }
+  if (mode != FKNN_MODE_EXACT_FP32) {
+    set_error("fknn_search: mode not built into this index");
+    return FKNN_EUNSUPPORTED;
+  }
+  std::lock_guard<std::mutex> lock(idx->mu);
+  FKNN_CUDA(cudaSetDevice(idx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  const float *d_q = qvecs, *d_meta = metas;
+  uint32_t *d_ids = ids;
+  float *d_dists = dists;
+  const bool q_dev = is_device_ptr(qvecs), m_dev = is_device_ptr(metas);
+  const bool i_dev = is_device_ptr(ids), dd_dev = dists ? is_device_ptr(dists) : true;
+  if (!q_dev) {
+    if ((rc = ws_get(idx, 0, (size_t)nq * DIM * 4, (void **)&d_q))) return rc;
+    FKNN_CUDA(cudaMemcpyAsync((void *)d_q, qvecs, (size_t)nq * DIM * 4, cudaMemcpyHostToDevice, st));
+  }
+  if (!m_dev) {
+    if ((rc = ws_get(idx, 1, (size_t)nq * 16, (void **)&d_meta))) return rc;
+    FKNN_CUDA(cudaMemcpyAsync((void *)d_meta, metas, (size_t)nq * 16, cudaMemcpyHostToDevice, st));
+  }
+  if (!i_dev)
+    if ((rc = ws_get(idx, 8, (size_t)nq * k * 4, (void **)&d_ids))) return rc;
+  if (dists && !dd_dev)
+    if ((rc = ws_get(idx, 9, (size_t)nq * k * 4, (void **)&d_dists))) return rc;
+  rc = search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
+  if (rc) return rc;
+  if (!i_dev) FKNN_CUDA(cudaMemcpyAsync(ids, d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
+  if (dists && !dd_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_dists, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  int flag = 0;
+  FKNN_CUDA(cudaMemcpy(&flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  if (flag & (1 << 8)) {
+    set_error("fknn_search: a bounded device wait gave up; affected queries were answered by the exact scan");
+  }
+  if (stats) stats->kernel_launches = g_launches;
+  return FKNN_OK;
+}
+
+int fknn_search(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k, int mode,
+                uint32_t *ids, float *dists, void *stream) {
+  fknn_search_opts o;
+  o.mode = mode;
+  o.kprime = 0;
+  return fknn_search_ex(index, qvecs, metas, nq, k, &o, ids, dists, stream, nullptr);
+}
+
+int fknn_count_matches(fknn_index *idx, const float *metas, uint32_t nq, uint32_t *counts, void *stream) {
+  g_err.clear();
+  g_launches = 0;
+  if (!idx || !metas || !counts) return FKNN_EINVAL;
+  if (nq == 0) return FKNN_OK;
+  std::lock_guard<std::mutex> lock(idx->mu);
+  FKNN_CUDA(cudaSetDevice(idx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  const float *d_meta = metas;
+  uint32_t *d_c = counts;
+  const bool m_dev = is_device_ptr(metas), c_dev = is_device_ptr(counts);
+  if (!m_dev) {
+    if ((rc = ws_get(idx, 1, (size_t)nq * 16, (void **)&d_meta))) return rc;
+    FKNN_CUDA(cudaMemcpyAsync((void *)d_meta, metas, (size_t)nq * 16, cudaMemcpyHostToDevice, st));
+  }
+  if (!c_dev)
+    if ((rc = ws_get(idx, 8, (size_t)nq * 4, (void **)&d_c))) return rc;
+  // reuse the query validator with a zero vector block is not needed: only metas
+  if ((rc = count_matches(idx, d_meta, nq, d_c, st))) return rc;
+  if (!c_dev) FKNN_CUDA(cudaMemcpyAsync(counts, d_c, (size_t)nq * 4, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  return FKNN_OK;
+}
+
+int fknn_filter_rows(fknn_index *idx, const float *meta4, uint32_t *out_ids, uint64_t *count, void *stream) {
+  g_err.clear();
+  g_launches = 0;
+  if (!idx || !meta4 || !out_ids || !count) return FKNN_EINVAL;
+  const float t = meta4[0];
+  if (!(t == 0.f || t == 1.f || t == 2.f || t == 3.f)) {
+    set_error("fknn_filter_rows: query type not in {0,1,2,3}");
+    return FKNN_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(idx->mu);
+  FKNN_CUDA(cudaSetDevice(idx->device));
+  cudaStream_t st = (cudaStream_t)stream;
+  int rc;
+  uint32_t *d_out = out_ids;
+  const bool o_dev = is_device_ptr(out_ids);
+  if (!o_dev)
+    if ((rc = ws_get(idx, 8, (size_t)idx->n * 4, (void **)&d_out))) return rc;
+  if ((rc = filter_rows(idx, meta4, d_out, count, st))) return rc;
+  if (!o_dev && *count) FKNN_CUDA(cudaMemcpyAsync(out_ids, d_out, *count * 4, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  return FKNN_OK;
+}
+
+int fknn_bruteforce_rows(const float *nodes, uint32_t n, const float *queries, uint32_t nq, uint32_t *gt) {
+  g_err.clear();
+  if (!nodes || !queries || !gt || n == 0) {
+    set_error("fknn_bruteforce_rows: bad arguments");
+    return FKNN_EINVAL;
+  }
+  // split the contest rows into the columns the index takes
+  std::vector<float> vecs((size_t)n * DIM), labels(n), ts(n), qv((size_t)nq * DIM), meta((size_t)nq * 4);
+  for (uint32_t i = 0; i < n; ++i) {
+    const float *r = nodes + (size_t)i * (DIM + 2);
+    labels[i] = r[0];
+    ts[i] = r[1];
+    std::memcpy(&vecs[(size_t)i * DIM], r + 2, DIM * 4);
+  }
+  for (uint32_t i = 0; i < nq; ++i) {
+    const float *r = queries + (size_t)i * (DIM + 4);
+    std::memcpy(&meta[(size_t)i * 4], r, 16);
+    std::memcpy(&qv[(size_t)i * DIM], r + 4, DIM * 4);
+  }
+  fknn_index *idx = nullptr;
+  fknn_index_opts o;
+  std::memset(&o, 0, sizeof(o));
+  int rc = fknn_index_create(vecs.data(), labels.data(), ts.data(), n, DIM, &o, &idx);
+  if (rc) return rc;
+  rc = fknn_search(idx, qv.data(), meta.data(), nq, 100, FKNN_MODE_EXACT_FP32, gt, nullptr, nullptr);
+  std::string keep = g_err;
+  fknn_index_destroy(idx);
+  g_err = keep;
+  return rc;
+}
+
+}  // extern "C"

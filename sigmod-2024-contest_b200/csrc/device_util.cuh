@@ -1,0 +1,174 @@
+// Small device helpers: mbarrier + bulk-copy PTX, bounded waits, sorts,
+// the reference's sequential L2.
+#pragma once
+
+#include "fknn_internal.cuh"
+
+namespace fknn {
+
+// Iteration cap for every spin-wait (~ a second or two at B200 clocks).
+constexpr uint32_t WAIT_LIMIT = 1u << 26;
+
+// Error bits written to the per-call device flag.
+constexpr int ERR_WAIT_TIMEOUT = 1 << 8;
+constexpr int ERR_BAD_QUERY_TYPE = 1 << 0;
+constexpr int ERR_BAD_QUERY_VALUE = 1 << 1;
+constexpr int ERR_BAD_QUERY_VEC = 1 << 2;
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+__device__ __forceinline__ void fence_mbar_init() {
+  asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+
+__device__ __forceinline__ void fence_proxy_async() {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t *bar, uint32_t bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+}
+
+// 1-D bulk copy global -> shared (the TMA bulk engine), completion counted
+// on an mbarrier.  dst, src 16-byte aligned; bytes a multiple of 16.
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, uint32_t bytes, uint64_t *bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+          smem_u32(dst)),
+      "l"(src), "r"(bytes), "r"(smem_u32(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
+  uint32_t ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_u32(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait: returns false (and raises ERR_WAIT_TIMEOUT) if the phase
+// never completes.
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+    if (mbar_try_wait(bar, parity)) return true;
+  atomicOr(err, ERR_WAIT_TIMEOUT);
+  return false;
+}
+
+__device__ __forceinline__ uint32_t ld_volatile_u32(const uint32_t *p) { return *(const volatile uint32_t *)p; }
+
+// distance.h:62-72 normal_l2(base, query): v = x - q; v *= v; r += v, every
+// operation rounded to float, in dimension order, never fused.
+__device__ __forceinline__ float seq_l2_strided(const float *x, int xstride, const float *q) {
+  float r = 0.f;
+#pragma unroll 10
+  for (int d = 0; d < DIM; ++d) {
+    float v = __fsub_rn(x[d * xstride], q[d]);
+    v = __fmul_rn(v, v);
+    r = __fadd_rn(r, v);
+  }
+  return r;
+}
+
+__device__ __forceinline__ uint64_t exact_key(float d, uint32_t id) {
+  return ((uint64_t)f32_sortable(d) << 32) | id;
+}
+
+// In-shared-memory bitonic sort of n (power of two) elements, ascending,
+// all threads of the block participate.
+template <typename K>
+__device__ void block_bitonic_sort(K *key, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < (n >> 1); i += blockDim.x) {
+        int lo = 2 * stride * (i / stride) + (i % stride);
+        int hi = lo + stride;
+        bool asc = (lo & size) == 0;
+        K a = key[lo], b = key[hi];
+        if ((a > b) == asc) {
+          key[lo] = b;
+          key[hi] = a;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Key/value variant ordered by (key, val).
+template <typename K, typename V>
+__device__ void block_bitonic_sort_kv(K *key, V *val, int n) {
+  for (int size = 2; size <= n; size <<= 1) {
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      for (int i = threadIdx.x; i < (n >> 1); i += blockDim.x) {
+        int lo = 2 * stride * (i / stride) + (i % stride);
+        int hi = lo + stride;
+        bool asc = (lo & size) == 0;
+        K a = key[lo], b = key[hi];
+        V va = val[lo], vb = val[hi];
+        bool gt = (a > b) || (a == b && va > vb);
+        if (gt == asc) {
+          key[lo] = b;
+          key[hi] = a;
+          val[lo] = vb;
+          val[hi] = va;
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// Warp-wide bitonic sort of 32*N (key, val) pairs held N per lane, element
+// e = j*32 + lane in register j, ascending by (key, val).
+template <int N>
+__device__ __forceinline__ void warp_bitonic_sort(float (&key)[N], uint32_t (&val)[N]) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int size = 2; size <= 32 * N; size <<= 1) {
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      if (stride >= 32) {
+        const int rs = stride >> 5;
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          const int p = j ^ rs;
+          if (p > j) {
+            const bool asc = (((j << 5) | lane) & size) == 0;
+            const bool gt = key[j] > key[p] || (key[j] == key[p] && val[j] > val[p]);
+            if (gt == asc) {
+              float tk = key[j]; key[j] = key[p]; key[p] = tk;
+              uint32_t tv = val[j]; val[j] = val[p]; val[p] = tv;
+            }
+          }
+        }
+      } else {
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+          const float ok = __shfl_xor_sync(0xffffffffu, key[j], stride);
+          const uint32_t ov = __shfl_xor_sync(0xffffffffu, val[j], stride);
+          const bool asc = (((j << 5) | lane) & size) == 0;
+          const bool lower = (lane & stride) == 0;
+          const bool other_less = ok < key[j] || (ok == key[j] && ov < val[j]);
+          const bool take_other = (lower == asc) ? other_less : !other_less && !(ok == key[j] && ov == val[j]);
+          if (take_other) {
+            key[j] = ok;
+            val[j] = ov;
+          }
+        }
+      }
+    }
+  }
+}
+
+}  // namespace fknn

@@ -1,0 +1,1015 @@
+// Exact FP32 filtered top-k (the B200 form of utils.h:80-158 Bruteforce).
+//
+// Pipeline for one batch of queries:
+//   1. k_query_prep   predicate -> contiguous slab [s, e) of one row order
+//                     (binary search on the sorted attribute columns), ||q||^2
+//   2. host planner   slabs <= SMALL_SLAB -> row-by-row exact scan; others
+//                     sorted and grouped into 64-query tiles, split into
+//                     (tile, row chunk) work items
+//   3. k_tile_stage   query tiles in the [101][64] layout of the base blocks
+//   4. k_screen       FP32 FFMA contraction q.x over 64-row blocks streamed by
+//                     the TMA bulk engine; ds = |x|^2+|q|^2-2q.x; rows whose
+//                     ds can still reach the running k-th bound are kept in a
+//                     per-(item, query) candidate list that a warp bitonic
+//                     sort compacts; the bound is shared across CTAs.
+//   5. k_merge        per query: union of its items' lists, k-th bound, then
+//                     exact re-score of the survivors with the reference's
+//                     sequential arithmetic, (dist, id) sort, top-k out.
+//   6. k_exact_scan   small slabs and any query whose candidates overflowed:
+//                     exact distances row by row, block select on (dist, id).
+// Ids and distances equal the reference's bit for bit: every row that can
+// be in the top k (screening error bound in screen_eps) is re-scored with
+// normal_l2's exact operation sequence and ordered by (dist, id) like the
+// ResultMaxHeap of utils.h:35-78.
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "device_util.cuh"
+
+namespace fknn {
+
+namespace {
+
+// ---------------------------------------------------------------- prep --
+
+__device__ __forceinline__ uint32_t lower_bound_i32(const int32_t *a, uint32_t lo, uint32_t hi, int32_t v) {
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (a[m] < v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+__device__ __forceinline__ uint32_t upper_bound_i32(const int32_t *a, uint32_t lo, uint32_t hi, int32_t v) {
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (a[m] <= v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+// first position with ts >= v
+__device__ __forceinline__ uint32_t lower_bound_f32(const float *a, uint32_t lo, uint32_t hi, float v) {
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (a[m] < v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+// first position with ts > v
+__device__ __forceinline__ uint32_t upper_bound_f32(const float *a, uint32_t lo, uint32_t hi, float v) {
+  while (lo < hi) {
+    uint32_t m = lo + ((hi - lo) >> 1);
+    if (a[m] <= v) lo = m + 1; else hi = m;
+  }
+  return lo;
+}
+
+// Query checks: type in {0,1,2,3} (searcher.hpp:39-42 rejects the rest),
+// v inside int32 for types 1/3 (read as int32, utils.h:99), window bounds
+// not NaN for types 2/3, vector values finite and <= 1e15.
+__global__ void k_validate_queries(const float *__restrict__ q, const float *__restrict__ meta, uint32_t nq,
+                                   int *flag) {
+  const uint64_t total = (uint64_t)nq * DIM;
+  int bad = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total;
+       i += (uint64_t)gridDim.x * blockDim.x) {
+    if (!(fabsf(q[i]) <= 1e15f)) bad |= ERR_BAD_QUERY_VEC;
+    if (i < nq) {
+      const float *m = meta + i * 4;
+      float t = m[0];
+      if (!(t == 0.f || t == 1.f || t == 2.f || t == 3.f)) bad |= ERR_BAD_QUERY_TYPE;
+      if ((t == 1.f || t == 3.f) && !(fabsf(m[1]) < 2147483648.f)) bad |= ERR_BAD_QUERY_VALUE;
+      if ((t == 2.f || t == 3.f) && (m[2] != m[2] || m[3] != m[3])) bad |= ERR_BAD_QUERY_VALUE;
+    }
+  }
+  if (bad) atomicOr(flag, bad);
+}
+
+// Predicate -> slab.  type 0: all rows (time order); 1: label == v (category
+// order); 2: l <= ts <= r (time order); 3: both (category order, the window
+// inside the label's slab).  The semantics are utils.h:110-137's.
+__device__ __forceinline__ void resolve_slab(const float *m, uint32_t n, const float *ts_t, const int32_t *lab_c,
+                                             const float *ts_c, int32_t &order, uint32_t &s, uint32_t &e) {
+  const uint32_t type = (uint32_t)m[0];
+  if (type == 0) {
+    order = ORDER_TIME; s = 0; e = n;
+  } else if (type == 2) {
+    order = ORDER_TIME;
+    s = lower_bound_f32(ts_t, 0, n, m[2]);
+    e = upper_bound_f32(ts_t, 0, n, m[3]);
+  } else {
+    order = ORDER_CAT;
+    const int32_t v = (int32_t)m[1];
+    s = lower_bound_i32(lab_c, 0, n, v);
+    e = upper_bound_i32(lab_c, s, n, v);
+    if (type == 3) {
+      uint32_t cs = s, ce = e;
+      s = lower_bound_f32(ts_c, cs, ce, m[2]);
+      e = upper_bound_f32(ts_c, cs, ce, m[3]);
+    }
+  }
+  if (e < s) e = s;
+}
+
+__global__ void k_query_prep(const float *__restrict__ q, const float *__restrict__ meta, uint32_t nq, uint32_t n,
+                             const float *__restrict__ ts_t, const int32_t *__restrict__ lab_c,
+                             const float *__restrict__ ts_c, QueryDesc *__restrict__ desc) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  QueryDesc dsc;
+  resolve_slab(meta + (uint64_t)i * 4, n, ts_t, lab_c, ts_c, dsc.order, dsc.s, dsc.e);
+  const float *v = q + (uint64_t)i * DIM;
+  float s = 0.f;
+#pragma unroll 10
+  for (int d = 0; d < DIM; ++d) s = fmaf(v[d], v[d], s);
+  dsc.qn = s;
+  desc[i] = dsc;
+}
+
+__global__ void k_count(const float *__restrict__ meta, uint32_t nq, uint32_t n, const float *__restrict__ ts_t,
+                        const int32_t *__restrict__ lab_c, const float *__restrict__ ts_c,
+                        uint32_t *__restrict__ counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= nq) return;
+  int32_t o;
+  uint32_t s, e;
+  resolve_slab(meta + (uint64_t)i * 4, n, ts_t, lab_c, ts_c, o, s, e);
+  counts[i] = e - s;
+}
+
+// Query tiles in the base-block layout: [101][64] (dims, then |q|^2).
+__global__ void k_tile_stage(const float *__restrict__ q, const QueryDesc *__restrict__ desc,
+                             const int32_t *__restrict__ lane_q, float *__restrict__ qtiles) {
+  const uint32_t t = blockIdx.x;
+  __shared__ float tile[TQ][DIM + 1];
+  for (int i = threadIdx.x; i < TQ * DIM; i += blockDim.x) {
+    int l = i / DIM, d = i % DIM;
+    int32_t qi = lane_q[t * TQ + l];
+    tile[l][d] = qi >= 0 ? q[(uint64_t)qi * DIM + d] : 0.f;
+  }
+  __syncthreads();
+  float *out = qtiles + (uint64_t)t * BLK_FLOATS;
+  for (int i = threadIdx.x; i < TQ * DIM; i += blockDim.x) {
+    int d = i / TQ, l = i % TQ;
+    out[d * TQ + l] = tile[l][d];
+  }
+  for (int l = threadIdx.x; l < TQ; l += blockDim.x) {
+    int32_t qi = lane_q[t * TQ + l];
+    out[DIM * TQ + l] = qi >= 0 ? desc[qi].qn : 0.f;
+  }
+}
+
+// -------------------------------------------------------------- screen --
+
+constexpr int SC_THREADS = 128;
+constexpr int SC_STAGES = 3;
+constexpr int SC_REFRESH = 16;  // sub-tiles between reads of the shared bound
+
+struct ScreenSmem {
+  float qs[BLK_FLOATS];
+  float xs[SC_STAGES][BLK_FLOATS];
+  float push[TQ];     // largest ds worth keeping
+  float thr[TQ];      // current upper bound T on the k-th distance
+  float qn[TQ];
+  int cnt[TQ];
+  uint32_t ls[TQ], le[TQ];
+  int32_t lq[TQ];
+  uint64_t bar[SC_STAGES + 1];
+};
+
+// Sort, bound and trim one (item, query) candidate list.  Whole warp.
+__device__ void compact_list(Candidate *list, ScreenSmem &sm, int L, uint32_t k, uint32_t *T_global,
+                             uint32_t *ovf) {
+  const int lane = threadIdx.x & 31;
+  const int n = sm.cnt[L];
+  float key[CAP / 32];
+  uint32_t val[CAP / 32];
+#pragma unroll
+  for (int j = 0; j < CAP / 32; ++j) {
+    int e = j * 32 + lane;
+    if (e < n) {
+      Candidate c = list[e];
+      key[j] = c.ds;
+      val[j] = c.pos;
+    } else {
+      key[j] = INFINITY;
+      val[j] = 0xffffffffu;
+    }
+  }
+  warp_bitonic_sort<CAP / 32>(key, val);
+  const float qn = sm.qn[L];
+  const int32_t qi = sm.lq[L];
+  float T = sm.thr[L];
+  if (n >= (int)k) {
+    const int e = (int)k - 1;
+    float mine = key[0];
+#pragma unroll
+    for (int j = 1; j < CAP / 32; ++j)
+      if (j == (e >> 5)) mine = key[j];
+    const float kth = __shfl_sync(0xffffffffu, mine, e & 31);
+    T = fminf(T, screen_hi(kth, qn));
+  }
+  const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+  if (Tg < T) T = Tg;
+  if (lane == 0 && T < Tg) atomicMin(T_global + qi, f32_sortable(T));
+  int kept = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int j = 0; j < CAP / 32; ++j) {
+    const bool keep = (j * 32 + lane) < n && screen_lo(key[j], qn) <= T;
+    const uint32_t b = __ballot_sync(0xffffffffu, keep);
+    if (keep) {
+      Candidate c;
+      c.ds = key[j];
+      c.pos = val[j];
+      list[kept + __popc(b & lt)] = c;
+    }
+    kept += __popc(b);
+  }
+  __syncwarp();
+  if (lane == 0) {
+    if (kept > CAP - BLK) {
+      // More near-ties than the list can hold: hand the query to the exact scan.
+      ovf[qi] = 1u;
+      sm.cnt[L] = 0;
+      sm.thr[L] = -INFINITY;
+      sm.push[L] = -INFINITY;
+    } else {
+      sm.cnt[L] = kept;
+      sm.thr[L] = T;
+      sm.push[L] = (T == INFINITY) ? INFINITY : screen_push_limit(T, qn);
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(SC_THREADS, 2)
+    k_screen(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles, const float *__restrict__ qtiles,
+             const int32_t *__restrict__ lane_q, const uint32_t *__restrict__ lane_s,
+             const uint32_t *__restrict__ lane_e, const float *__restrict__ blocks_t,
+             const float *__restrict__ blocks_c, uint32_t *__restrict__ T_global, uint32_t *__restrict__ ovf,
+             Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt, uint32_t k, int *err) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  ScreenSmem &sm = *reinterpret_cast<ScreenSmem *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t item_id = blockIdx.x;
+  const WorkItem it = items[item_id];
+  const Tile tl = tiles[it.tile];
+  const float *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
+  const uint32_t nsub = it.blk1 - it.blk0;
+  Candidate *out_item = out + (uint64_t)item_id * TQ * CAP;
+
+  if (tid == 0) {
+    for (int s = 0; s < SC_STAGES + 1; ++s) mbar_init(&sm.bar[s], 1);
+    fence_mbar_init();
+  }
+  __syncthreads();
+  if (tid == 0) {
+    mbar_arrive_expect_tx(&sm.bar[SC_STAGES], BLK_BYTES);
+    bulk_g2s(sm.qs, qtiles + (uint64_t)it.tile * BLK_FLOATS, BLK_BYTES, &sm.bar[SC_STAGES]);
+    for (uint32_t s = 0; s < SC_STAGES && s < nsub; ++s) {
+      mbar_arrive_expect_tx(&sm.bar[s], BLK_BYTES);
+      bulk_g2s(sm.xs[s], blocks + (uint64_t)(it.blk0 + s) * BLK_FLOATS, BLK_BYTES, &sm.bar[s]);
+    }
+  }
+  // every wait's outcome is made block-uniform before any barrier depends on it
+  bool ok = __syncthreads_and(mbar_wait_bounded(&sm.bar[SC_STAGES], 0, err)) != 0;
+  if (tid < TQ) {
+    const int32_t qi = lane_q[it.tile * TQ + tid];
+    sm.lq[tid] = qi;
+    sm.cnt[tid] = 0;
+    sm.qn[tid] = sm.qs[DIM * TQ + tid];
+    if (qi >= 0) {
+      sm.ls[tid] = lane_s[it.tile * TQ + tid];
+      sm.le[tid] = lane_e[it.tile * TQ + tid];
+      const float T = sortable_f32(ld_volatile_u32(T_global + qi));
+      sm.thr[tid] = T;
+      sm.push[tid] = (T == INFINITY) ? INFINITY : screen_push_limit(T, sm.qn[tid]);
+      if (ld_volatile_u32(ovf + qi)) sm.push[tid] = -INFINITY;
+    } else {
+      sm.ls[tid] = sm.le[tid] = 0;
+      sm.thr[tid] = -INFINITY;
+      sm.push[tid] = -INFINITY;
+    }
+  }
+  __syncthreads();
+
+  const int ty = tid & 15;  // rows ty*4 .. ty*4+3 of the 64-row block
+  const int tx = tid >> 4;  // queries tx*8 .. tx*8+7 of the tile
+  for (uint32_t sub = 0; sub < nsub && ok; ++sub) {
+    const int st = sub % SC_STAGES;
+    if (!__syncthreads_and(mbar_wait_bounded(&sm.bar[st], (sub / SC_STAGES) & 1, err))) {
+      ok = false;
+      break;
+    }
+    const float *xs = sm.xs[st];
+    float acc[4][8];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
+    const float4 *xr = reinterpret_cast<const float4 *>(xs) + ty;
+    const float4 *qr = reinterpret_cast<const float4 *>(sm.qs) + tx * 2;
+#pragma unroll 20
+    for (int d = 0; d < DIM; ++d) {
+      const float4 a = xr[d * (BLK / 4)];
+      const float4 b0 = qr[d * (TQ / 4)];
+      const float4 b1 = qr[d * (TQ / 4) + 1];
+      const float av[4] = {a.x, a.y, a.z, a.w};
+      const float bv[8] = {b0.x, b0.y, b0.z, b0.w, b1.x, b1.y, b1.z, b1.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
+    }
+    // epilogue: ds = (|x|^2 + |q|^2) - 2 q.x, keep rows that can reach the bound
+    const float4 xn4 = reinterpret_cast<const float4 *>(xs + DIM * BLK)[ty];
+    const float xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
+    const uint32_t row0 = (it.blk0 + sub) * BLK + ty * 4;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int L = tx * 8 + j;
+      const float pl = sm.push[L];
+      const float qn = sm.qn[L];
+      const uint32_t s = sm.ls[L], e = sm.le[L];
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float ds = fmaf(-2.f, acc[i][j], xn[i] + qn);
+        const uint32_t p = row0 + i;
+        if (ds <= pl && p >= s && p < e) {
+          const int idx = atomicAdd(&sm.cnt[L], 1);
+          Candidate c;
+          c.ds = ds;
+          c.pos = p;
+          out_item[(uint64_t)L * CAP + idx] = c;
+        }
+      }
+    }
+    __syncthreads();
+    if (tid == 0 && sub + SC_STAGES < nsub) {
+      fence_proxy_async();
+      mbar_arrive_expect_tx(&sm.bar[st], BLK_BYTES);
+      bulk_g2s(sm.xs[st], blocks + (uint64_t)(it.blk0 + sub + SC_STAGES) * BLK_FLOATS, BLK_BYTES, &sm.bar[st]);
+    }
+    // lists near capacity are compacted; bounds refreshed from other CTAs
+    const bool refresh = (sub % SC_REFRESH) == SC_REFRESH - 1;
+    {
+      const int L = warp + 4 * (lane & 15);
+      const bool need = lane < 16 && sm.cnt[L] > CAP - BLK;
+      uint32_t m = __ballot_sync(0xffffffffu, need);
+      while (m) {
+        const int b = __ffs(m) - 1;
+        m &= m - 1;
+        compact_list(out_item + (uint64_t)(warp + 4 * b) * CAP, sm, warp + 4 * b, k, T_global, ovf);
+      }
+      if (refresh && lane < 16 && !need) {
+        const int32_t qi = sm.lq[L];
+        if (qi >= 0 && sm.push[L] != -INFINITY) {
+          const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+          if (Tg < sm.thr[L]) {
+            sm.thr[L] = Tg;
+            sm.push[L] = screen_push_limit(Tg, sm.qn[L]);
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  if (!ok) {
+    // A bulk copy never landed (bounded wait gave up): give the copies still
+    // in flight a second bounded wait, then mark every query of the tile so
+    // the exact scan answers them.
+    if (tid == 0) {
+      for (uint32_t s = 0; s < SC_STAGES && s < nsub; ++s) {
+        for (uint32_t itr = 0; itr < WAIT_LIMIT; ++itr)
+          if (mbar_try_wait(&sm.bar[s], 0) && mbar_try_wait(&sm.bar[s], 1)) break;
+      }
+    }
+    if (tid < TQ && sm.lq[tid] >= 0) ovf[sm.lq[tid]] = 1u;
+    __syncthreads();
+    if (tid < TQ) out_cnt[(uint64_t)item_id * TQ + tid] = 0;
+    return;
+  }
+  // final trim of every non-empty list
+  for (int b = 0; b < 16; ++b) {
+    const int L = warp + 4 * b;
+    if (sm.cnt[L] > 0) compact_list(out_item + (uint64_t)L * CAP, sm, L, k, T_global, ovf);
+  }
+  __syncthreads();
+  if (tid < TQ) out_cnt[(uint64_t)item_id * TQ + tid] = (uint32_t)sm.cnt[tid];
+}
+
+// --------------------------------------------------------------- merge --
+
+constexpr int MG_THREADS = 256;
+
+struct MergeSmem {
+  float key[MERGE_CAP];
+  uint32_t val[MERGE_CAP];
+  uint64_t ekey[RESCORE_CAP];
+  float qv[DIM];
+  uint32_t cnt_prefix[MG_THREADS + 1];
+  int total, surv, status;
+};
+
+__global__ void __launch_bounds__(MG_THREADS)
+    k_merge(const uint32_t *__restrict__ big_q, const uint32_t *__restrict__ big_tile,
+            const uint32_t *__restrict__ big_lane, const Tile *__restrict__ tiles, const uint32_t *__restrict__ item_slot,
+            const Candidate *__restrict__ out,
+            const uint32_t *__restrict__ out_cnt, const QueryDesc *__restrict__ desc, const float *__restrict__ q,
+            const float *__restrict__ vecs, const uint32_t *__restrict__ perm_t, const uint32_t *__restrict__ perm_c,
+            const uint32_t *__restrict__ T_global, const uint32_t *__restrict__ ovf, uint32_t *__restrict__ ovf_list,
+            uint32_t *__restrict__ ovf_count, uint32_t k, uint32_t *__restrict__ ids, float *__restrict__ dists) {
+  extern __shared__ __align__(128) unsigned char smem_raw[];
+  MergeSmem &sm = *reinterpret_cast<MergeSmem *>(smem_raw);
+  const int tid = threadIdx.x;
+  const uint32_t qi = big_q[blockIdx.x];
+  if (ovf[qi]) {
+    if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
+    return;
+  }
+  const Tile tl = tiles[big_tile[blockIdx.x]];
+  const uint32_t L = big_lane[blockIdx.x];
+  const uint32_t nitems = tl.item1 - tl.item0;
+  const QueryDesc dsc = desc[qi];
+  const float qn = dsc.qn;
+  for (int d = tid; d < DIM; d += MG_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
+  // 1. gather the lists (per-thread strip of items, block prefix)
+  const uint32_t per = (nitems + MG_THREADS - 1) / MG_THREADS;
+  const uint32_t ib = tid * per, ie = min(ib + per, nitems);
+  uint32_t mine = 0;
+  for (uint32_t i = ib; i < ie; ++i) mine += out_cnt[(uint64_t)item_slot[tl.item0 + i] * TQ + L];
+  sm.cnt_prefix[tid + 1] = mine;
+  if (tid == 0) sm.cnt_prefix[0] = 0;
+  __syncthreads();
+  if (tid == 0) {
+    for (int t = 0; t < MG_THREADS; ++t) sm.cnt_prefix[t + 1] += sm.cnt_prefix[t];
+    sm.total = (int)sm.cnt_prefix[MG_THREADS];
+  }
+  __syncthreads();
+  const int M = sm.total;
+  if (M > MERGE_CAP) {
+    if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
+    return;
+  }
+  {
+    uint32_t w = sm.cnt_prefix[tid];
+    for (uint32_t i = ib; i < ie; ++i) {
+      const uint64_t item = item_slot[tl.item0 + i];
+      const uint32_t c = out_cnt[item * TQ + L];
+      const Candidate *src = out + (item * TQ + L) * CAP;
+      for (uint32_t j = 0; j < c; ++j) {
+        Candidate cd = src[j];
+        sm.key[w] = cd.ds;
+        sm.val[w] = cd.pos;
+        ++w;
+      }
+    }
+  }
+  int np2 = 32;
+  while (np2 < M) np2 <<= 1;
+  for (int i = M + tid; i < np2; i += MG_THREADS) {
+    sm.key[i] = INFINITY;
+    sm.val[i] = 0xffffffffu;
+  }
+  __syncthreads();
+  // 2. k-th bound over the union
+  block_bitonic_sort_kv(sm.key, sm.val, np2);
+  float T = sortable_f32(T_global[qi]);
+  if (M >= (int)k) T = fminf(T, screen_hi(sm.key[k - 1], qn));
+  // 3. survivors (a prefix of the sorted list up to rounding; scan anyway)
+  if (tid == 0) sm.surv = 0;
+  __syncthreads();
+  for (int i = tid; i < M; i += MG_THREADS) {
+    if (screen_lo(sm.key[i], qn) <= T) {
+      int slot = atomicAdd(&sm.surv, 1);
+      if (slot < RESCORE_CAP) {
+        const uint32_t pos = sm.val[i];
+        const uint32_t id = (dsc.order == ORDER_TIME ? perm_t : perm_c)[pos];
+        sm.ekey[slot] = (uint64_t)id;  // re-scored below
+      }
+    }
+  }
+  __syncthreads();
+  const int S = sm.surv;
+  if (S > RESCORE_CAP) {
+    if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
+    return;
+  }
+  // 4. exact re-score (distance.h:62-72 order of operations)
+  for (int i = tid; i < S; i += MG_THREADS) {
+    const uint32_t id = (uint32_t)sm.ekey[i];
+    const float d = seq_l2_strided(vecs + (uint64_t)id * DIM, 1, sm.qv);
+    sm.ekey[i] = exact_key(d, id);
+  }
+  int sp2 = 32;
+  while (sp2 < S) sp2 <<= 1;
+  for (int i = S + tid; i < sp2; i += MG_THREADS) sm.ekey[i] = ~0ull;
+  __syncthreads();
+  block_bitonic_sort(sm.ekey, sp2);
+  for (uint32_t j = tid; j < k; j += MG_THREADS) {
+    uint32_t id = 0xffffffffu;
+    float d = INFINITY;
+    if ((int)j < S) {
+      id = (uint32_t)sm.ekey[j];
+      d = sortable_f32((uint32_t)(sm.ekey[j] >> 32));
+    }
+    ids[(uint64_t)qi * k + j] = id;
+    if (dists) dists[(uint64_t)qi * k + j] = d;
+  }
+}
+
+// ----------------------------------------------------------- exact scan --
+
+constexpr int ES_THREADS = 256;
+constexpr int ES_CAP = 1024;
+
+__global__ void __launch_bounds__(ES_THREADS)
+    k_exact_scan(const uint32_t *__restrict__ list, const uint32_t *__restrict__ d_count, uint32_t h_count,
+                 const QueryDesc *__restrict__ desc, const float *__restrict__ q, const float *__restrict__ blocks_t,
+                 const float *__restrict__ blocks_c, const uint32_t *__restrict__ perm_t,
+                 const uint32_t *__restrict__ perm_c, uint32_t k, uint32_t *__restrict__ ids,
+                 float *__restrict__ dists) {
+  __shared__ uint64_t buf[ES_CAP];
+  __shared__ float qv[DIM];
+  __shared__ int cnt;
+  __shared__ uint64_t thr;
+  const uint32_t count = d_count ? *d_count : h_count;
+  const int tid = threadIdx.x;
+  for (uint32_t li = blockIdx.x; li < count; li += gridDim.x) {
+    const uint32_t qi = list[li];
+    const QueryDesc dsc = desc[qi];
+    const float *blocks = dsc.order == ORDER_TIME ? blocks_t : blocks_c;
+    const uint32_t *perm = dsc.order == ORDER_TIME ? perm_t : perm_c;
+    for (int d = tid; d < DIM; d += ES_THREADS) qv[d] = q[(uint64_t)qi * DIM + d];
+    if (tid == 0) {
+      cnt = 0;
+      thr = ~0ull;
+    }
+    __syncthreads();
+    for (uint64_t base = dsc.s; base < dsc.e; base += ES_THREADS) {
+      const uint64_t p = base + tid;
+      if (p < dsc.e) {
+        const float *x = blocks + (p / BLK) * BLK_FLOATS + (p % BLK);
+        const float d = seq_l2_strided(x, BLK, qv);
+        const uint64_t key = exact_key(d, perm[p]);
+        if (key < thr) buf[atomicAdd(&cnt, 1)] = key;
+      }
+      __syncthreads();
+      if (cnt > ES_CAP - ES_THREADS) {
+        for (int i = cnt + tid; i < ES_CAP; i += ES_THREADS) buf[i] = ~0ull;
+        __syncthreads();
+        block_bitonic_sort(buf, ES_CAP);
+        if (tid == 0) {
+          cnt = (int)k;
+          thr = buf[k - 1];
+        }
+        __syncthreads();
+      }
+    }
+    int c = cnt;
+    int np2 = 32;
+    while (np2 < c) np2 <<= 1;
+    for (int i = c + tid; i < np2; i += ES_THREADS) buf[i] = ~0ull;
+    __syncthreads();
+    block_bitonic_sort(buf, np2);
+    for (uint32_t j = tid; j < k; j += ES_THREADS) {
+      uint32_t id = 0xffffffffu;
+      float d = INFINITY;
+      if ((int)j < c) {
+        id = (uint32_t)buf[j];
+        d = sortable_f32((uint32_t)(buf[j] >> 32));
+      }
+      ids[(uint64_t)qi * k + j] = id;
+      if (dists) dists[(uint64_t)qi * k + j] = d;
+    }
+    __syncthreads();
+  }
+}
+
+// ------------------------------------------------- predicate compaction --
+
+constexpr int FC_THREADS = 256;
+constexpr int FC_ITEMS = 16;
+constexpr int FC_TILE = FC_THREADS * FC_ITEMS;
+
+__device__ __forceinline__ bool row_passes(uint32_t type, int32_t v, float l, float r, float label, float ts) {
+  switch (type) {
+    case 0: return true;
+    case 1: return (int32_t)label == v;
+    case 2: return ts >= l && ts <= r;
+    default: return (int32_t)label == v && ts >= l && ts <= r;
+  }
+}
+
+// Pass 1: passing rows per 4096-row tile (warp ballots, coalesced columns).
+__global__ void k_filter_count(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n,
+                               float4 m, uint32_t *__restrict__ tile_cnt) {
+  __shared__ uint32_t wsum[FC_THREADS / 32];
+  const uint32_t type = (uint32_t)m.x;
+  const int32_t v = (int32_t)m.y;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * FC_TILE;
+  uint32_t c = 0;
+  for (int i = 0; i < FC_ITEMS; ++i) {
+    const uint64_t idx = base + (uint64_t)i * FC_THREADS + threadIdx.x;
+    const bool p = idx < n && row_passes(type, v, m.z, m.w, labels[idx], ts[idx]);
+    c += __popc(__ballot_sync(0xffffffffu, p));
+  }
+  if (lane == 0) wsum[w] = c;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    uint32_t s = 0;
+    for (int i = 0; i < FC_THREADS / 32; ++i) s += wsum[i];
+    tile_cnt[blockIdx.x] = s;
+  }
+}
+
+// Pass 2 (after an exclusive scan of tile_cnt): write passing ids in order.
+__global__ void k_filter_write(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n, float4 m,
+                               const uint32_t *__restrict__ tile_off, uint32_t *__restrict__ out) {
+  __shared__ uint32_t wcnt[FC_THREADS / 32];
+  __shared__ uint32_t run;
+  const uint32_t type = (uint32_t)m.x;
+  const int32_t v = (int32_t)m.y;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  const uint64_t base = (uint64_t)blockIdx.x * FC_TILE;
+  if (threadIdx.x == 0) run = tile_off[blockIdx.x];
+  __syncthreads();
+  for (int i = 0; i < FC_ITEMS; ++i) {
+    const uint64_t idx = base + (uint64_t)i * FC_THREADS + threadIdx.x;
+    const bool p = idx < n && row_passes(type, v, m.z, m.w, labels[idx], ts[idx]);
+    const uint32_t b = __ballot_sync(0xffffffffu, p);
+    if (lane == 0) wcnt[w] = __popc(b);
+    __syncthreads();
+    uint32_t before = run;
+    for (int ww = 0; ww < w; ++ww) before += wcnt[ww];
+    if (p) out[before + __popc(b & ((1u << lane) - 1u))] = (uint32_t)idx;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      uint32_t s = 0;
+      for (int ww = 0; ww < FC_THREADS / 32; ++ww) s += wcnt[ww];
+      run += s;
+    }
+    __syncthreads();
+  }
+}
+
+__global__ void k_exclusive_scan_small(uint32_t *data, uint32_t len, uint32_t *total) {
+  // single thread; len is N/4096 (a few thousand)
+  uint32_t s = 0;
+  for (uint32_t i = 0; i < len; ++i) {
+    uint32_t v = data[i];
+    data[i] = s;
+    s += v;
+  }
+  *total = s;
+}
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+// ============================================================== host side
+
+int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st) {
+  int *flag = idx->d_flag;
+  FKNN_CUDA(cudaMemsetAsync(flag, 0, sizeof(int), st));
+  unsigned grid = (unsigned)std::min<uint64_t>(((uint64_t)nq * DIM + 255) / 256, 148 * 8);
+  if (grid == 0) grid = 1;
+  k_validate_queries<<<grid, 256, 0, st>>>(d_q, d_meta, nq, flag);
+  g_launches += 1;
+  return FKNN_OK;
+}
+
+static int check_query_flag(int flag) {
+  if (!flag) return FKNN_OK;
+  std::string m = "fknn_search: ";
+  if (flag & ERR_BAD_QUERY_TYPE) m += "query type not in {0,1,2,3}; ";
+  if (flag & ERR_BAD_QUERY_VALUE) m += "query category outside int32 or NaN window bound; ";
+  if (flag & ERR_BAD_QUERY_VEC) m += "query vector value not finite or above 1e15; ";
+  set_error(m);
+  return FKNN_EINVAL;
+}
+
+int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d_counts, cudaStream_t st) {
+  if (nq == 0) return FKNN_OK;
+  k_count<<<(nq + 255) / 256, 256, 0, st>>>(d_meta, nq, (uint32_t)idx->n, idx->ord[ORDER_TIME].ts,
+                                           idx->ord[ORDER_CAT].label, idx->ord[ORDER_CAT].ts, d_counts);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *count, cudaStream_t st) {
+  const uint64_t n = idx->n;
+  const uint32_t ntiles = (uint32_t)((n + FC_TILE - 1) / FC_TILE);
+  uint32_t *tc;
+  int rc = ws_get(idx, 10, (size_t)(ntiles + 1) * 4, (void **)&tc);
+  if (rc) return rc;
+  const float4 m = make_float4(m4[0], m4[1], m4[2], m4[3]);
+  k_filter_count<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc);
+  k_exclusive_scan_small<<<1, 1, 0, st>>>(tc, ntiles, tc + ntiles);
+  k_filter_write<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc, d_out);
+  g_launches += 3;
+  uint32_t tot = 0;
+  FKNN_CUDA(cudaMemcpyAsync(&tot, tc + ntiles, 4, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  *count = tot;
+  return FKNN_OK;
+}
+
+namespace {
+
+struct Plan {
+  std::vector<uint32_t> small;                 // query ids for the exact scan
+  std::vector<uint32_t> big, big_tile, big_lane;
+  std::vector<Tile> tiles;
+  std::vector<WorkItem> items;
+  std::vector<int32_t> lane_q;
+  std::vector<uint32_t> lane_s, lane_e;
+  uint64_t pairs_screened = 0, pairs_passing = 0, pairs_contraction = 0;
+};
+
+// Groups queries into 64-query tiles whose slabs overlap (same order and
+// predicate class, start bucket, then end), and cuts each tile's union
+// range into row chunks.
+void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, Plan &P) {
+  std::vector<uint32_t> big;
+  big.reserve(nq);
+  for (uint32_t i = 0; i < nq; ++i) {
+    const uint32_t len = desc[i].e - desc[i].s;
+    P.pairs_passing += len;
+    if (len <= (uint32_t)SMALL_SLAB) {
+      P.small.push_back(i);
+    } else {
+      big.push_back(i);
+      P.pairs_contraction += len;
+    }
+  }
+  if (big.empty()) return;
+  // start buckets: about sqrt(#queries/64) per class so a tile spans little
+  const uint64_t nb_all = std::max<uint64_t>(1, (uint64_t)std::sqrt((double)big.size() / 64.0));
+  const uint64_t bw = std::max<uint64_t>(BLK, (n + nb_all - 1) / nb_all);
+  struct Key {
+    uint32_t order, cls;
+    uint64_t bucket;
+    uint32_t s, e, qi;
+  };
+  std::vector<Key> keys(big.size());
+  for (size_t j = 0; j < big.size(); ++j) {
+    const uint32_t i = big[j];
+    const QueryDesc &d = desc[i];
+    Key kk;
+    kk.order = (uint32_t)d.order;
+    kk.cls = (uint32_t)meta_host[(size_t)i * 4];
+    kk.bucket = (kk.cls == 2 || kk.cls == 3) ? d.s / bw : 0;
+    kk.s = d.s;
+    kk.e = d.e;
+    kk.qi = i;
+    keys[j] = kk;
+  }
+  std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
+    if (a.order != b.order) return a.order < b.order;
+    if (a.cls != b.cls) return a.cls < b.cls;
+    if (a.bucket != b.bucket) return a.bucket < b.bucket;
+    if (a.e != b.e) return a.e < b.e;
+    if (a.s != b.s) return a.s < b.s;
+    return a.qi < b.qi;
+  });
+  // greedy tiles
+  struct TileTmp {
+    uint32_t first, count, S, E, order;
+  };
+  std::vector<TileTmp> tt;
+  size_t i = 0;
+  while (i < keys.size()) {
+    TileTmp t{(uint32_t)i, 1, keys[i].s, keys[i].e, keys[i].order};
+    uint32_t maxlen = keys[i].e - keys[i].s;
+    size_t j = i + 1;
+    while (j < keys.size() && t.count < TQ && keys[j].order == keys[i].order && keys[j].cls == keys[i].cls &&
+           keys[j].bucket == keys[i].bucket) {
+      const uint32_t S = std::min(t.S, keys[j].s), E = std::max(t.E, keys[j].e);
+      const uint32_t ml = std::max(maxlen, keys[j].e - keys[j].s);
+      if ((uint64_t)(E - S) > (uint64_t)ml + std::max<uint64_t>(ml / 3, 8192)) break;
+      t.S = S;
+      t.E = E;
+      maxlen = ml;
+      ++t.count;
+      ++j;
+    }
+    tt.push_back(t);
+    i = j;
+  }
+  // chunk size from the total work: aim for >= ~8 items per resident CTA
+  uint64_t total_blk = 0;
+  for (auto &t : tt) total_blk += (t.E + BLK - 1) / BLK - t.S / BLK;
+  uint64_t cb = total_blk / (148ull * 2 * 8);
+  cb = std::max<uint64_t>(16, std::min<uint64_t>(1024, cb));
+  const size_t ntile = tt.size();
+  P.tiles.resize(ntile);
+  P.lane_q.assign(ntile * TQ, -1);
+  P.lane_s.assign(ntile * TQ, 0);
+  P.lane_e.assign(ntile * TQ, 0);
+  P.big.reserve(big.size());
+  P.big_tile.reserve(big.size());
+  P.big_lane.reserve(big.size());
+  std::vector<WorkItem> items;
+  for (size_t t = 0; t < ntile; ++t) {
+    const TileTmp &T = tt[t];
+    for (uint32_t l = 0; l < T.count; ++l) {
+      const Key &kk = keys[T.first + l];
+      P.lane_q[t * TQ + l] = (int32_t)kk.qi;
+      P.lane_s[t * TQ + l] = kk.s;
+      P.lane_e[t * TQ + l] = kk.e;
+      P.big.push_back(kk.qi);
+      P.big_tile.push_back((uint32_t)t);
+      P.big_lane.push_back(l);
+    }
+    const uint32_t b0 = T.S / BLK, b1 = (T.E + BLK - 1) / BLK;
+    P.tiles[t].order = (int32_t)T.order;
+    P.tiles[t].nq = T.count;
+    for (uint32_t b = b0; b < b1; b += (uint32_t)cb) {
+      WorkItem w;
+      w.tile = (uint32_t)t;
+      w.blk0 = b;
+      w.blk1 = std::min<uint32_t>(b1, b + (uint32_t)cb);
+      w.pad = 0;
+      items.push_back(w);
+      P.pairs_screened += (uint64_t)(w.blk1 - w.blk0) * BLK * TQ;
+    }
+  }
+  // Launch order: items that read the same rows run side by side (L2
+  // reuse).  A tile's items are then spread out; the merge finds them
+  // through the per-tile slot table built in search_exact.
+  std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
+    if (P.tiles[a.tile].order != P.tiles[b.tile].order) return P.tiles[a.tile].order < P.tiles[b.tile].order;
+    return a.blk0 < b.blk0;
+  });
+  std::vector<uint32_t> per_tile(ntile + 1, 0);
+  for (auto &w : items) per_tile[w.tile + 1]++;
+  for (size_t t = 0; t < ntile; ++t) per_tile[t + 1] += per_tile[t];
+  for (size_t t = 0; t < ntile; ++t) {
+    P.tiles[t].item0 = per_tile[t];
+    P.tiles[t].item1 = per_tile[t + 1];
+  }
+  P.items = std::move(items);
+}
+
+}  // namespace
+
+int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
+                 float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  const uint64_t n = idx->n;
+  int rc;
+  // 1. validate + resolve slabs
+  QueryDesc *d_desc;
+  if ((rc = ws_get(idx, 2, (size_t)nq * sizeof(QueryDesc), (void **)&d_desc))) return rc;
+  if ((rc = validate_queries(idx, d_q, d_meta, nq, st))) return rc;
+  k_query_prep<<<(nq + 255) / 256, 256, 0, st>>>(d_q, d_meta, nq, (uint32_t)n, idx->ord[ORDER_TIME].ts,
+                                                 idx->ord[ORDER_CAT].label, idx->ord[ORDER_CAT].ts, d_desc);
+  g_launches += 1;
+  QueryDesc *h_desc;
+  float *h_meta;
+  int *h_flag;
+  if ((rc = hs_get(idx, 0, (size_t)nq * sizeof(QueryDesc), (void **)&h_desc))) return rc;
+  if ((rc = hs_get(idx, 1, (size_t)nq * 16, (void **)&h_meta))) return rc;
+  if ((rc = hs_get(idx, 2, 64, (void **)&h_flag))) return rc;
+  FKNN_CUDA(cudaMemcpyAsync(h_flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaMemcpyAsync(h_desc, d_desc, (size_t)nq * sizeof(QueryDesc), cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaMemcpyAsync(h_meta, d_meta, (size_t)nq * 16, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  if ((rc = check_query_flag(*h_flag))) return rc;
+
+  // 2. plan
+  auto t0 = std::chrono::steady_clock::now();
+  Plan P;
+  make_plan(h_desc, h_meta, nq, n, P);
+  auto t1 = std::chrono::steady_clock::now();
+  const uint32_t ntile = (uint32_t)P.tiles.size(), nitems = (uint32_t)P.items.size();
+  const uint32_t nbig = (uint32_t)P.big.size(), nsmall = (uint32_t)P.small.size();
+
+  // item slots: the merge reads a tile's lists through tile.item0..item1 of
+  // a slot table, the screen writes each item's lists at its launch slot.
+  std::vector<uint32_t> slot_of_tile_item(nitems);
+  {
+    std::vector<uint32_t> fill(ntile);
+    for (uint32_t t = 0; t < ntile; ++t) fill[t] = P.tiles[t].item0;
+    for (uint32_t s = 0; s < nitems; ++s) slot_of_tile_item[fill[P.items[s].tile]++] = s;
+  }
+
+  // 3. upload the plan as one blob
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = align_up(off + bytes, 256);
+    return o;
+  };
+  const size_t o_small = take(nsmall * 4), o_big = take(nbig * 4), o_btile = take(nbig * 4),
+               o_blane = take(nbig * 4), o_tiles = take(ntile * sizeof(Tile)), o_items = take(nitems * sizeof(WorkItem)),
+               o_lq = take((size_t)ntile * TQ * 4), o_ls = take((size_t)ntile * TQ * 4),
+               o_le = take((size_t)ntile * TQ * 4), o_slot = take(nitems * 4);
+  const size_t blob = off;
+  unsigned char *h_blob, *d_blob;
+  if ((rc = hs_get(idx, 3, blob + 256, (void **)&h_blob))) return rc;
+  if ((rc = ws_get(idx, 3, blob + 256, (void **)&d_blob))) return rc;
+  auto put = [&](size_t o, const void *src, size_t bytes) {
+    if (bytes) std::memcpy(h_blob + o, src, bytes);
+  };
+  put(o_small, P.small.data(), nsmall * 4);
+  put(o_big, P.big.data(), nbig * 4);
+  put(o_btile, P.big_tile.data(), nbig * 4);
+  put(o_blane, P.big_lane.data(), nbig * 4);
+  put(o_tiles, P.tiles.data(), ntile * sizeof(Tile));
+  put(o_items, P.items.data(), nitems * sizeof(WorkItem));
+  put(o_lq, P.lane_q.data(), (size_t)ntile * TQ * 4);
+  put(o_ls, P.lane_s.data(), (size_t)ntile * TQ * 4);
+  put(o_le, P.lane_e.data(), (size_t)ntile * TQ * 4);
+  put(o_slot, slot_of_tile_item.data(), nitems * 4);
+  if (blob) FKNN_CUDA(cudaMemcpyAsync(d_blob, h_blob, blob, cudaMemcpyHostToDevice, st));
+
+  // per-query state: bound, overflow flag, overflow list + count
+  uint32_t *d_state;
+  if ((rc = ws_get(idx, 5, (size_t)nq * 12 + 64, (void **)&d_state))) return rc;
+  uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
+           *ovf_count = d_state + 3 * (size_t)nq;
+  FKNN_CUDA(cudaMemsetAsync(T_global, 0xff, (size_t)nq * 4, st));
+  FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
+  FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 4, st));
+
+  const OrderData &OT = idx->ord[ORDER_TIME], &OC = idx->ord[ORDER_CAT];
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (stats) {
+    for (auto &e : ev) FKNN_CUDA(cudaEventCreate(&e));
+  }
+  if (nitems) {
+    float *d_qt;
+    Candidate *d_out;
+    uint32_t *d_ocnt;
+    if ((rc = ws_get(idx, 4, (size_t)ntile * BLK_BYTES, (void **)&d_qt))) return rc;
+    if ((rc = ws_get(idx, 6, (size_t)nitems * TQ * CAP * sizeof(Candidate), (void **)&d_out))) return rc;
+    if ((rc = ws_get(idx, 7, (size_t)nitems * TQ * 4, (void **)&d_ocnt))) return rc;
+    k_tile_stage<<<ntile, 256, 0, st>>>(d_q, d_desc, (const int32_t *)(d_blob + o_lq), d_qt);
+    const size_t smem = sizeof(ScreenSmem);
+    static bool attr_set = false;
+    if (!attr_set) {
+      FKNN_CUDA(cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      FKNN_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MergeSmem)));
+      attr_set = true;
+    }
+    if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
+    k_screen<<<nitems, SC_THREADS, smem, st>>>(
+        (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_qt, (const int32_t *)(d_blob + o_lq),
+        (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), OT.blocks, OC.blocks, T_global, ovf,
+        d_out, d_ocnt, k, idx->d_flag);
+    if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
+    k_merge<<<nbig, MG_THREADS, sizeof(MergeSmem), st>>>(
+        (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
+        (const Tile *)(d_blob + o_tiles), (const uint32_t *)(d_blob + o_slot), d_out, d_ocnt, d_desc, d_q, idx->vecs,
+        OT.perm, OC.perm, T_global, ovf, ovf_list, ovf_count, k, d_ids, d_dists);
+    g_launches += 3;
+  }
+  if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));
+  if (nsmall) {
+    const unsigned grid = std::min<uint32_t>(nsmall, 148 * 8);
+    k_exact_scan<<<grid, ES_THREADS, 0, st>>>((const uint32_t *)(d_blob + o_small), nullptr, nsmall, d_desc, d_q,
+                                              OT.blocks, OC.blocks, OT.perm, OC.perm, k, d_ids, d_dists);
+    g_launches += 1;
+  }
+  if (nbig) {
+    k_exact_scan<<<148 * 2, ES_THREADS, 0, st>>>(ovf_list, ovf_count, 0, d_desc, d_q, OT.blocks, OC.blocks, OT.perm,
+                                                 OC.perm, k, d_ids, d_dists);
+    g_launches += 1;
+  }
+  FKNN_CUDA(cudaGetLastError());
+  if (stats) {
+    FKNN_CUDA(cudaEventRecord(ev[3], st));
+    FKNN_CUDA(cudaEventSynchronize(ev[3]));
+    float ms = 0.f;
+    if (nitems) {
+      FKNN_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      stats->ms_screen = ms;
+      FKNN_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+      stats->ms_merge = ms;
+    }
+    FKNN_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+    stats->ms_scan = ms;
+    for (auto &e : ev) cudaEventDestroy(e);
+    stats->pairs_screened = P.pairs_screened;
+    stats->pairs_passing = P.pairs_passing;
+    stats->pairs_contraction = P.pairs_contraction;
+    stats->n_tiles = ntile;
+    stats->n_work_items = nitems;
+    stats->n_small = nsmall;
+    stats->ms_plan = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    uint32_t h_ovf = 0;
+    FKNN_CUDA(cudaMemcpyAsync(&h_ovf, ovf_count, 4, cudaMemcpyDeviceToHost, st));
+    FKNN_CUDA(cudaStreamSynchronize(st));
+    stats->n_overflow = h_ovf;
+  }
+  return FKNN_OK;
+}
+
+}  // namespace fknn

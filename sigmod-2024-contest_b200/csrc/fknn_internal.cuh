@@ -1,0 +1,181 @@
+// Internal definitions shared by the fknn CUDA sources.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "fknn.h"
+
+namespace fknn {
+
+constexpr int DIM = FKNN_DIM;     // 100, utils.h:255
+constexpr int BLK = 64;           // rows per layout block
+constexpr int BLK_ROWS_F = DIM + 1;            // 100 dims + the row norm
+constexpr int BLK_FLOATS = BLK_ROWS_F * BLK;   // one block: [101][64] float
+constexpr uint32_t BLK_BYTES = BLK_FLOATS * 4; // 25856, a multiple of 16
+constexpr int TQ = 64;            // queries per contraction tile
+constexpr int CAP = 256;          // candidate slots per (work item, query)
+constexpr int KMAX_TILE = 128;    // largest k the contraction path serves
+constexpr int SMALL_SLAB = 4096;  // slabs up to this size go to the row-by-row exact scan
+constexpr int MERGE_CAP = 4096;   // candidates one merge block can hold
+constexpr int RESCORE_CAP = 512;  // survivors one merge block can re-score
+
+enum Order : int { ORDER_TIME = 0, ORDER_CAT = 1 };
+
+// ---- order-preserving integer images of floats and ints ----
+__host__ __device__ __forceinline__ uint32_t f32_bits(float f) {
+#ifdef __CUDA_ARCH__
+  return __float_as_uint(f);
+#else
+  uint32_t u;
+  __builtin_memcpy(&u, &f, 4);
+  return u;
+#endif
+}
+__host__ __device__ __forceinline__ float bits_f32(uint32_t u) {
+#ifdef __CUDA_ARCH__
+  return __uint_as_float(u);
+#else
+  float f;
+  __builtin_memcpy(&f, &u, 4);
+  return f;
+#endif
+}
+// Monotone map float -> uint32 (total order, -0 < +0; callers canonicalise -0).
+__host__ __device__ __forceinline__ uint32_t f32_sortable(float f) {
+  uint32_t u = f32_bits(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__host__ __device__ __forceinline__ float sortable_f32(uint32_t s) {
+  uint32_t u = (s & 0x80000000u) ? (s & 0x7fffffffu) : ~s;
+  return bits_f32(u);
+}
+__host__ __device__ __forceinline__ uint32_t i32_sortable(int32_t v) { return (uint32_t)v ^ 0x80000000u; }
+
+// Screening error bound.  ds = ||x||^2 + ||q||^2 - 2 q.x, every sum a
+// float FMA chain over 100 terms, differs from the exact real distance by at
+// most gamma_101 (sqrt(xn)+sqrt(qn))^2 + u|ds|, and the reference's
+// sequential float sum (distance.h:62-72) differs from it by at most
+// gamma_102 * d.  With sqrt(xn) <= sqrt(d) + sqrt(qn) both are bounded by a
+// function of ds and qn alone; the constants below carry a factor > 1.5 of
+// slack over gamma_104 = 6.2e-6 (u = 2^-24).
+__host__ __device__ __forceinline__ float screen_eps(float ds, float qn) {
+  float D = fmaxf(ds, 0.f) * 1.0001f + 1e-4f * qn;
+  float a = sqrtf(D) + 2.f * sqrtf(qn);
+  return 2e-5f * a * a + 1e-5f * D + 1e-30f;
+}
+__host__ __device__ __forceinline__ float screen_lo(float ds, float qn) { return ds - screen_eps(ds, qn); }
+__host__ __device__ __forceinline__ float screen_hi(float ds, float qn) {
+  float h = ds + screen_eps(ds, qn);
+  return h + fabsf(h) * 1e-6f + 1e-30f;
+}
+// Largest ds whose lower bound can still reach T (a safe over-estimate).
+__host__ __device__ __forceinline__ float screen_push_limit(float T, float qn) {
+  float e = screen_eps(T + 2.f * screen_eps(T, qn), qn);
+  return T + e * 1.01f + fabsf(T) * 1e-6f;
+}
+
+// Per-query slab after predicate resolution.
+struct QueryDesc {
+  int32_t order;  // ORDER_TIME or ORDER_CAT
+  uint32_t s, e;  // rows [s, e) of that order pass the predicate
+  float qn;       // ||q||^2 as a float FMA chain
+};
+
+// One contraction work item: rows [blk0*64, blk1*64) of the tile's order.
+struct WorkItem {
+  uint32_t tile;
+  uint32_t blk0, blk1;
+  uint32_t pad;
+};
+
+struct Tile {
+  int32_t order;
+  uint32_t item0, item1;  // its work items
+  uint32_t nq;
+};
+
+struct Candidate {
+  float ds;
+  uint32_t pos;
+};
+
+// Device data of one row order.
+struct OrderData {
+  float *blocks = nullptr;     // [nblk][101][64]
+  uint32_t *perm = nullptr;    // [n] position -> row id
+  float *ts = nullptr;         // [n] timestamps in this order
+  int32_t *label = nullptr;    // [n] int32 labels in this order
+};
+
+// Grow-only device arena for per-call scratch.
+struct DevBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+struct HostBuf {
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+}  // namespace fknn
+
+struct fknn_index {
+  int device = 0;
+  uint64_t n = 0;
+  uint32_t nblk = 0;
+  float *vecs = nullptr;    // [n][100] row-major, original order
+  float *norms = nullptr;   // [n]
+  float *labels_f = nullptr;
+  float *ts_f = nullptr;
+  fknn::OrderData ord[2];
+  uint64_t bytes = 0;
+  uint64_t hbm_budget = 0;
+  // reduced-precision copies (built on request)
+  void *bf16_blocks[2] = {nullptr, nullptr};
+  void *fp8_blocks[2] = {nullptr, nullptr};
+  float *fp8_scale = nullptr;
+  // per-call scratch
+  std::mutex mu;
+  fknn::DevBuf ws[16];
+  fknn::HostBuf hs[8];
+  int *d_flag = nullptr;
+  cudaStream_t own_stream = nullptr;
+};
+
+namespace fknn {
+
+// error plumbing
+void set_error(const std::string &msg);
+int cuda_fail(cudaError_t e, const char *what);
+#define FKNN_CUDA(call)                                  \
+  do {                                                   \
+    cudaError_t _e = (call);                             \
+    if (_e != cudaSuccess) return ::fknn::cuda_fail(_e, #call); \
+  } while (0)
+
+int dev_alloc(fknn_index *idx, void **p, size_t bytes);
+int ws_get(fknn_index *idx, int slot, size_t bytes, void **p);
+int hs_get(fknn_index *idx, int slot, size_t bytes, void **p);
+
+// index build (index_build.cu)
+int build_index(fknn_index *idx, const float *vecs, const float *labels, const float *ts, cudaStream_t st);
+int radix_sort_pairs(fknn_index *idx, uint32_t *keys, uint32_t *vals, uint32_t *keys_tmp, uint32_t *vals_tmp,
+                     uint64_t n, int begin_bit, int end_bit, cudaStream_t st);
+
+// exact search (exact_search.cu)
+int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
+                 float *d_dists, cudaStream_t st, fknn_search_stats *stats);
+int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d_counts, cudaStream_t st);
+int filter_rows(fknn_index *idx, const float *meta4_host, uint32_t *d_out, uint64_t *count, cudaStream_t st);
+int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st);
+
+// launch counter (kernels launched by this library in the current call)
+extern thread_local uint32_t g_launches;
+
+}  // namespace fknn

@@ -1,0 +1,122 @@
+"""ctypes binding of libfknn.so (the C ABI declared in include/fknn.h).
+
+The shared library is built in-tree by ``make -C sigmod-2024-contest_b200``
+(or ``__graft_entry__.build()``).  There is no fallback: if the library is
+missing or fails to load, importing a search entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from ctypes import (POINTER, Structure, c_char_p, c_float, c_int, c_int8, c_size_t, c_uint32, c_uint64,
+                    c_void_p)
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "libfknn.so")
+
+FKNN_OK = 0
+FKNN_EINVAL = -1
+FKNN_ENOMEM = -2
+FKNN_ECUDA = -3
+FKNN_ETIMEOUT = -4
+FKNN_EUNSUPPORTED = -5
+FKNN_ENODEV = -6
+
+MODE_EXACT_FP32 = 0
+MODE_BF16_RERANK = 1
+MODE_FP8_RERANK = 2
+
+_ERRNAMES = {
+    FKNN_EINVAL: "FKNN_EINVAL",
+    FKNN_ENOMEM: "FKNN_ENOMEM",
+    FKNN_ECUDA: "FKNN_ECUDA",
+    FKNN_ETIMEOUT: "FKNN_ETIMEOUT",
+    FKNN_EUNSUPPORTED: "FKNN_EUNSUPPORTED",
+    FKNN_ENODEV: "FKNN_ENODEV",
+}
+
+
+class FknnError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{_ERRNAMES.get(code, code)}: {msg}")
+        self.code = code
+
+
+class IndexOpts(Structure):
+    _fields_ = [("device", c_int), ("build_bf16", c_int), ("build_fp8", c_int), ("hbm_budget", c_uint64)]
+
+
+class SearchOpts(Structure):
+    _fields_ = [("mode", c_int), ("kprime", c_uint32)]
+
+
+class SearchStats(Structure):
+    _fields_ = [
+        ("pairs_screened", c_uint64),
+        ("pairs_passing", c_uint64),
+        ("pairs_contraction", c_uint64),
+        ("n_tiles", c_uint32),
+        ("n_work_items", c_uint32),
+        ("n_small", c_uint32),
+        ("n_overflow", c_uint32),
+        ("n_boundary_f64", c_uint32),
+        ("kernel_launches", c_uint32),
+        ("ms_plan", c_float),
+        ("ms_screen", c_float),
+        ("ms_merge", c_float),
+        ("ms_scan", c_float),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
+# Every entry point of include/fknn.h with its ctypes signature.
+SIGNATURES = {
+    "fknn_version": (c_int, []),
+    "fknn_last_error": (c_char_p, []),
+    "fknn_index_create": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_uint32, POINTER(IndexOpts),
+                                  POINTER(c_void_p)]),
+    "fknn_index_destroy": (c_int, [c_void_p]),
+    "fknn_index_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "fknn_search": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p, c_void_p, c_void_p]),
+    "fknn_search_ex": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, POINTER(SearchOpts), c_void_p,
+                               c_void_p, c_void_p, POINTER(SearchStats)]),
+    "fknn_count_matches": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
+    "fknn_filter_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), c_void_p]),
+    "fknn_bruteforce_rows": (c_int, [c_void_p, c_uint32, c_void_p, c_uint32, c_void_p]),
+    "fknn_sq8_sym_train": (c_int, [c_void_p, c_uint64, POINTER(c_float), c_void_p]),
+    "fknn_sq8_sym_encode": (c_int, [c_void_p, c_uint64, c_float, c_void_p]),
+    "fknn_sq8_bruteforce": (c_int, [c_size_t, c_size_t, c_void_p, c_size_t, c_void_p, c_float, c_size_t, c_void_p]),
+    "fknn_sq8_bruteforce_subgraph": (c_int, [c_size_t, c_size_t, c_void_p, c_void_p, c_size_t, c_void_p, c_float,
+                                             c_size_t, c_void_p]),
+}
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Loads libfknn.so once; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libfknn.so is not built ({LIB_PATH}); build it with "
+                           f"`make -C {os.path.dirname(_HERE)}` or __graft_entry__.build()")
+    lib = ctypes.CDLL(LIB_PATH)
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != FKNN_OK:
+        msg = load().fknn_last_error()
+        raise FknnError(rc, msg.decode() if msg else "")
+
+
+def last_error() -> str:
+    return load().fknn_last_error().decode()

@@ -1,0 +1,216 @@
+"""Host-side mirror of the reference's filtered-kNN entry points over the C ABI.
+
+Reference interfaces mirrored (paths inside KevinZeng08/sigmod-2024-contest):
+  Bruteforce(nodes, queries, gt)                      utils.h:80-158
+  bruteforce(dim, k, closest_points, npoints, ...)    bruteforce.h:244-265
+  bruteforce_subgraph(..., distances, ...)            bruteforce.h:267-289
+  SQ8SymmetricQuantizer.train / encode                pyglass/glass/quant/sq8_sym_quant.hpp:32-74
+plus the resident-index form (Index) that the batch path uses.
+
+Arrays may be numpy (host) or torch tensors (host or CUDA); torch CUDA tensors
+are passed to the library as device pointers and stay on the device.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_float, c_uint64, c_void_p
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import (MODE_BF16_RERANK, MODE_EXACT_FP32, MODE_FP8_RERANK, IndexOpts, SearchOpts, SearchStats, check,
+                   load)
+
+DIM = 100
+K = 100  # utils.h:88
+SQ8_CODE = 112  # code_size = d aligned to 16 (sq8_sym_quant.hpp:27)
+
+
+def _is_torch(x) -> bool:
+    return type(x).__module__.startswith("torch")
+
+
+def _ptr(x, dtype) -> int:
+    """Address of a contiguous array of the given numpy dtype (numpy or torch)."""
+    if x is None:
+        return None
+    if _is_torch(x):
+        import torch
+        tdt = {np.float32: torch.float32, np.uint32: torch.int32, np.int32: torch.int32, np.int8: torch.int8,
+               np.float64: torch.float64}[np.dtype(dtype).type]
+        if x.dtype != tdt and not (tdt == torch.int32 and x.dtype == torch.uint32):
+            raise TypeError(f"expected a {tdt} tensor, got {x.dtype}")
+        if not x.is_contiguous():
+            raise ValueError("tensor must be contiguous")
+        return x.data_ptr()
+    if not isinstance(x, np.ndarray) or x.dtype != np.dtype(dtype) or not x.flags.c_contiguous:
+        raise TypeError(f"expected a C-contiguous numpy array of {np.dtype(dtype)}")
+    return x.ctypes.data
+
+
+def _stream_of(*xs) -> Optional[int]:
+    for x in xs:
+        if x is not None and _is_torch(x) and x.is_cuda:
+            import torch
+            return torch.cuda.current_stream(x.device).cuda_stream
+    return None
+
+
+class Index:
+    """Resident filtered-kNN index on one GPU (fknn_index_create).
+
+    vecs: (n, 100) float32, labels: (n,) float32 category (read as int32),
+    ts: (n,) float32 timestamp.  Row position is the id.
+    """
+
+    def __init__(self, vecs, labels, ts, device: int = 0, build_bf16: bool = False, build_fp8: bool = False,
+                 hbm_budget: int = 0):
+        lib = load()
+        vecs = np.ascontiguousarray(vecs, dtype=np.float32)
+        labels = np.ascontiguousarray(labels, dtype=np.float32)
+        ts = np.ascontiguousarray(ts, dtype=np.float32)
+        n = labels.shape[0]
+        if vecs.shape != (n, DIM) or ts.shape != (n,):
+            raise ValueError("vecs must be (n, 100), labels and ts (n,)")
+        opts = IndexOpts(device, int(build_bf16), int(build_fp8), hbm_budget)
+        h = c_void_p()
+        check(lib.fknn_index_create(vecs.ctypes.data, labels.ctypes.data, ts.ctypes.data, n, DIM, byref(opts),
+                                    byref(h)))
+        self._h = h
+        self.n = n
+        self.device = device
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().fknn_index_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    @property
+    def device_bytes(self) -> int:
+        b = c_uint64()
+        check(load().fknn_index_bytes(self._h, byref(b)))
+        return b.value
+
+    def search(self, qvecs, metas, k: int = K, mode: int = MODE_EXACT_FP32, ids=None, dists=None,
+               kprime: int = 0, with_dists: bool = True, stream: Optional[int] = None, return_stats: bool = False):
+        """Filtered top-k.  metas rows are (type, v, l, r) as in utils.h:98-101.
+
+        Returns (ids, dists) as numpy arrays for host inputs, or the given /
+        newly allocated torch CUDA tensors for device inputs.
+        """
+        lib = load()
+        dev = _is_torch(qvecs) and qvecs.is_cuda
+        nq = qvecs.shape[0]
+        if ids is None:
+            if dev:
+                import torch
+                ids = torch.empty((nq, k), dtype=torch.int32, device=qvecs.device)
+                dists = torch.empty((nq, k), dtype=torch.float32, device=qvecs.device) if with_dists else None
+            else:
+                qvecs = np.ascontiguousarray(qvecs, dtype=np.float32)
+                metas = np.ascontiguousarray(metas, dtype=np.float32)
+                ids = np.empty((nq, k), dtype=np.uint32)
+                dists = np.empty((nq, k), dtype=np.float32) if with_dists else None
+        if stream is None:
+            stream = _stream_of(qvecs, metas, ids)
+        opts = SearchOpts(mode, kprime)
+        st = SearchStats()
+        check(lib.fknn_search_ex(self._h, _ptr(qvecs, np.float32), _ptr(metas, np.float32), nq, k, byref(opts),
+                                 _ptr(ids, np.uint32), _ptr(dists, np.float32) if dists is not None else None,
+                                 stream, byref(st)))
+        if return_stats:
+            return ids, dists, st.as_dict()
+        return ids, dists
+
+    def count_matches(self, metas) -> np.ndarray:
+        metas = np.ascontiguousarray(metas, dtype=np.float32)
+        out = np.empty(metas.shape[0], dtype=np.uint32)
+        check(load().fknn_count_matches(self._h, metas.ctypes.data, metas.shape[0], out.ctypes.data, None))
+        return out
+
+    def filter_rows(self, meta4) -> np.ndarray:
+        """Ids of the rows passing one predicate (type, v, l, r), increasing."""
+        m = np.ascontiguousarray(meta4, dtype=np.float32).reshape(4)
+        out = np.empty(self.n, dtype=np.uint32)
+        cnt = c_uint64()
+        check(load().fknn_filter_rows(self._h, m.ctypes.data, out.ctypes.data, byref(cnt), None))
+        return out[: cnt.value].copy()
+
+
+def Bruteforce(nodes, queries, gt: Optional[list] = None):
+    """utils.h:80 Bruteforce: nodes rows (label, ts, 100 dims), queries rows
+    (type, v, l, r, 100 dims) -> gt[nq][100] ascending (distance, id).
+
+    Unlike the reference, queries with fewer than 100 passing rows do not
+    throw; their tail is UINT32_MAX.  Returns gt (filled in place when a list
+    is given).
+    """
+    nodes_a = np.ascontiguousarray(np.asarray(nodes, dtype=np.float32))
+    q_a = np.ascontiguousarray(np.asarray(queries, dtype=np.float32))
+    if nodes_a.ndim != 2 or nodes_a.shape[1] != DIM + 2 or q_a.ndim != 2 or q_a.shape[1] != DIM + 4:
+        raise ValueError("nodes must be (n, 102) and queries (nq, 104)")
+    out = np.empty((q_a.shape[0], K), dtype=np.uint32)
+    check(load().fknn_bruteforce_rows(nodes_a.ctypes.data, nodes_a.shape[0], q_a.ctypes.data, q_a.shape[0],
+                                      out.ctypes.data))
+    if gt is not None:
+        gt.clear()
+        gt.extend(list(map(int, r)) for r in out)
+        return gt
+    return out
+
+
+class SQ8SymmetricQuantizer:
+    """sq8_sym_quant.hpp: one global scale alpha = max|x|, int8 codes of 112 bytes."""
+
+    def __init__(self, dim: int = DIM):
+        if dim != DIM:
+            raise ValueError("dim must be 100")
+        self.d = dim
+        self.code_size = SQ8_CODE
+        self.alpha = 0.0
+        self.codes: Optional[np.ndarray] = None
+
+    def train(self, data, n: Optional[int] = None) -> None:
+        data = np.ascontiguousarray(data, dtype=np.float32).reshape(-1, DIM)
+        if n is not None:
+            data = data[:n]
+        codes = np.empty((data.shape[0], SQ8_CODE), dtype=np.int8)
+        a = c_float()
+        check(load().fknn_sq8_sym_train(data.ctypes.data, data.shape[0], byref(a), codes.ctypes.data))
+        self.alpha = a.value
+        self.codes = codes
+
+    def encode(self, vecs) -> np.ndarray:
+        v = np.ascontiguousarray(vecs, dtype=np.float32).reshape(-1, DIM)
+        out = np.empty((v.shape[0], SQ8_CODE), dtype=np.int8)
+        check(load().fknn_sq8_sym_encode(v.ctypes.data, v.shape[0], c_float(self.alpha), out.ctypes.data))
+        return out
+
+
+def bruteforce(dim: int, k: int, closest_points, npoints: int, codes_in, alpha: float, nqueries: int,
+               queries_in) -> None:
+    """bruteforce.h:244 with the same arguments; closest_points (nqueries*k
+    int32) is filled in the reference's heap-array order."""
+    check(load().fknn_sq8_bruteforce(dim, k, _ptr(closest_points, np.int32), npoints, _ptr(codes_in, np.int8),
+                                     c_float(alpha), nqueries, _ptr(queries_in, np.int8)))
+
+
+def bruteforce_subgraph(dim: int, k: int, closest_points, distances, npoints: int, codes_in, alpha: float,
+                        nqueries: int, queries_in) -> None:
+    """bruteforce.h:267: also distances[k] = heap distance * alpha * alpha."""
+    check(load().fknn_sq8_bruteforce_subgraph(dim, k, _ptr(closest_points, np.int32), _ptr(distances, np.float32),
+                                              npoints, _ptr(codes_in, np.int8), c_float(alpha), nqueries,
+                                              _ptr(queries_in, np.int8)))

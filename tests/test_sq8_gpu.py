@@ -1,0 +1,69 @@
+"""SQ8 symmetric quantizer and the SQ8 slab brute force on the GPU against
+the reference's outputs (golden fixture, heap-array order included) and the
+oracle restatement."""
+import os
+
+import numpy as np
+import pytest
+
+import fknn
+import oracle
+from fknn import datagen
+
+pytestmark = pytest.mark.gpu
+
+
+def test_train_encode_match_reference_fixture(golden_dir):
+    f = np.load(os.path.join(golden_dir, "sq8.npz"))
+    vecs, labels, ts, q, metas = datagen.make_workload(1, n=6000, nq=12)
+    quant = fknn.SQ8SymmetricQuantizer(100)
+    quant.train(vecs)
+    assert np.float32(quant.alpha) == f["alpha"]
+    _, ocodes = oracle.sq8_sym_train(vecs)
+    np.testing.assert_array_equal(quant.codes, ocodes)
+    np.testing.assert_array_equal(quant.encode(q), f["qcodes"])
+
+
+def test_bruteforce_heap_order_matches_reference_fixture(golden_dir):
+    f = np.load(os.path.join(golden_dir, "sq8.npz"))
+    vecs, labels, ts, q, metas = datagen.make_workload(1, n=6000, nq=12)
+    alpha, codes = oracle.sq8_sym_train(vecs)
+    qcodes = f["qcodes"]
+    tie_codes = np.repeat(codes[:700], 4, axis=0)
+    for j, (k, s, npnt, src) in enumerate(f["cases"]):
+        slab = np.ascontiguousarray((codes if src == 0 else tie_codes)[s:s + npnt])
+        k = int(k)
+        # one query per call, exactly as hybrid_graph.cpp:211 calls it
+        for i in range(qcodes.shape[0]):
+            out = np.empty(k, dtype=np.int32)
+            fknn.bruteforce(100, k, out, int(npnt), slab, alpha, 1, np.ascontiguousarray(qcodes[i]))
+            np.testing.assert_array_equal(out, f[f"ids{j}"][i])
+        # batched: all queries against the slab in one call, with distances
+        outb = np.empty((qcodes.shape[0], k), dtype=np.int32)
+        dist = np.empty((qcodes.shape[0], k), dtype=np.float32)
+        fknn.bruteforce_subgraph(100, k, outb, dist, int(npnt), slab, alpha, qcodes.shape[0], qcodes)
+        np.testing.assert_array_equal(outb, f[f"ids{j}"])
+        np.testing.assert_array_equal(dist, f[f"dists{j}"])
+
+
+@pytest.mark.parametrize("npoints,k", [(140, 140), (5000, 140), (200000, 140), (70000, 1), (30000, 1000)])
+def test_bruteforce_matches_oracle(npoints, k):
+    rng = np.random.default_rng(npoints + k)
+    base = rng.standard_normal((npoints // 3 + 1, 100), dtype=np.float32)
+    vecs = np.repeat(base, 3, axis=0)[:npoints]  # many equal distances
+    alpha, codes = oracle.sq8_sym_train(vecs)
+    qv = oracle.sq8_sym_encode(rng.standard_normal((5, 100), dtype=np.float32), alpha)
+    out = np.empty((5, k), dtype=np.int32)
+    d = np.empty((5, k), dtype=np.float32)
+    fknn.bruteforce_subgraph(100, k, out, d, npoints, codes, alpha, 5, qv)
+    for i in range(5):
+        oi, od = oracle.sq8_bruteforce(k, codes, alpha, qv[i], with_dists=True)
+        np.testing.assert_array_equal(out[i], oi)
+        np.testing.assert_array_equal(d[i], od)
+
+
+def test_bruteforce_rejects_bad_k():
+    codes = np.zeros((10, 112), np.int8)
+    out = np.empty(11, np.int32)
+    with pytest.raises(fknn.FknnError):
+        fknn.bruteforce(100, 11, out, 10, codes, 1.0, 1, np.zeros(112, np.int8))
