@@ -668,6 +668,10 @@ __global__ void k_exclusive_scan_small(uint32_t *data, uint32_t len, uint32_t *t
   *total = s;
 }
 
+__global__ void k_fill_u32(uint32_t *__restrict__ p, uint32_t n, uint32_t v) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) p[i] = v;
+}
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
@@ -831,11 +835,12 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
     const uint32_t b0 = T.S / BLK, b1 = (T.E + BLK - 1) / BLK;
     P.tiles[t].order = (int32_t)T.order;
     P.tiles[t].nq = T.count;
-    for (uint32_t b = b0; b < b1; b += (uint32_t)cb) {
+    const uint32_t cbt = std::max<uint32_t>((uint32_t)cb, (b1 - b0 + MAX_ITEMS_PER_TILE - 1) / MAX_ITEMS_PER_TILE);
+    for (uint32_t b = b0; b < b1; b += cbt) {
       WorkItem w;
       w.tile = (uint32_t)t;
       w.blk0 = b;
-      w.blk1 = std::min<uint32_t>(b1, b + (uint32_t)cb);
+      w.blk1 = std::min<uint32_t>(b1, b + cbt);
       w.pad = 0;
       items.push_back(w);
       P.pairs_screened += (uint64_t)(w.blk1 - w.blk0) * BLK * TQ;
@@ -935,7 +940,9 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
   if ((rc = ws_get(idx, 5, (size_t)nq * 12 + 64, (void **)&d_state))) return rc;
   uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
            *ovf_count = d_state + 3 * (size_t)nq;
-  FKNN_CUDA(cudaMemsetAsync(T_global, 0xff, (size_t)nq * 4, st));
+  // bounds start at +inf (as an order-preserving integer image)
+  k_fill_u32<<<std::min<uint32_t>((nq + 255) / 256, 1024), 256, 0, st>>>(T_global, nq, f32_sortable(INFINITY));
+  g_launches += 1;
   FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
   FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 4, st));
 

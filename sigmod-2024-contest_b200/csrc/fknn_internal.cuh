@@ -21,7 +21,8 @@ constexpr int TQ = 64;            // queries per contraction tile
 constexpr int CAP = 256;          // candidate slots per (work item, query)
 constexpr int KMAX_TILE = 128;    // largest k the contraction path serves
 constexpr int SMALL_SLAB = 4096;  // slabs up to this size go to the row-by-row exact scan
-constexpr int MERGE_CAP = 4096;   // candidates one merge block can hold
+constexpr int MERGE_CAP = 8192;   // candidates one merge block can hold
+constexpr int MAX_ITEMS_PER_TILE = 32;  // so a tile's lists (<= 32 x 192) always fit one merge
 constexpr int RESCORE_CAP = 512;  // survivors one merge block can re-score
 
 enum Order : int { ORDER_TIME = 0, ORDER_CAT = 1 };

@@ -21,11 +21,14 @@ def run(vecs, labels, ts, q, metas, k=100, **kw):
 
 
 def assert_same_as_oracle(vecs, labels, ts, q, metas, k=100):
-    ids, dists = run(vecs, labels, ts, q, metas, k=k)
+    with fknn.Index(vecs, labels, ts) as idx:
+        ids, dists, st = idx.search(q, metas, k=k, return_stats=True)
     oids, odists = oracle.exact_knn(vecs, labels, ts, q, metas, k=k)
     bad = np.nonzero(np.any(ids != oids, axis=1))[0]
     assert len(bad) == 0, f"{len(bad)} queries differ, first {bad[:5]}"
     np.testing.assert_array_equal(dists.view(np.uint32), odists.view(np.uint32))
+    # candidate lists only overflow into the exact scan on near-tie floods
+    assert st["n_overflow"] <= max(2, q.shape[0] // 50), st
     return ids, dists
 
 
@@ -181,8 +184,8 @@ def test_full_size_sampled_against_oracle():
         ids, dists, st = idx.search(q, metas, return_stats=True)
     assert st["n_overflow"] == 0
     valid = ids != UMAX
-    d = np.where(valid, dists, np.inf)
-    assert np.all(np.diff(d, axis=1) >= 0)
+    assert np.all(np.isinf(dists[~valid]))
+    assert np.all(dists[:, 1:] >= dists[:, :-1])  # ascending, +inf padding last
     rng = np.random.default_rng(11)
     sel = rng.choice(q.shape[0], 400, replace=False)
     oids, odists = oracle.exact_knn(vecs, labels, ts, q[sel], metas[sel])
