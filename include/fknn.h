@@ -119,6 +119,29 @@ int fknn_count_matches(fknn_index *index, const float *metas, uint32_t nq, uint3
  * order into out_ids (capacity n) and their number into *count. */
 int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, uint64_t *count, void *stream);
 
+/* No counterpart in the reference: the predicate evaluation + row compaction
+ * of fknn_filter_rows for callers that cannot allocate device memory -- code
+ * that runs under a fixed, pre-reserved HBM budget or a foreign memory pool
+ * where cudaMalloc is refused, and latency-critical paths where cudaMalloc's
+ * implicit device synchronisation is not acceptable.  It allocates nothing:
+ * no cudaMalloc, no cudaFree, no pinned staging, no index.
+ *   labels, ts : n float32 each, DEVICE memory of the current device, in the
+ *                caller's row order (the ids written are positions in them)
+ *   meta4      : HOST pointer to one predicate (type, v, l, r)
+ *   out_ids    : DEVICE memory of capacity n; passing row ids, increasing
+ *   count      : HOST pointer; receives the number of passing rows
+ * Limit: n <= 268,435,456 (65,536 tiles of 4,096 rows); larger n returns
+ * FKNN_EINVAL.  The per-tile counters live in one fixed 256 KiB device array
+ * that every GPU loading this library holds until the process exits; every
+ * call shares it and it keeps the last call's contents (each call rewrites
+ * all counters it reads).  Calls that overlap on the GPU (other streams,
+ * other host threads, same device) race on that array: serialise them.  The
+ * first call on a device looks up the array's device address (set-up once
+ * per device), so make that first call before any stream capture begins.
+ * The call waits for its stream before returning (the count is read back). */
+int fknn_filter_rows_noalloc(const float *labels, const float *ts, uint64_t n, const float *meta4,
+                             uint32_t *out_ids, uint64_t *count, void *stream);
+
 /* Drop-in for utils.h:80 Bruteforce on contest-layout rows: nodes n x 102
  * (label, ts, 100 dims), queries nq x 104 (type, v, l, r, 100 dims), gt
  * nq x 100 ascending (distance, id).  Builds a temporary index on device 0. */

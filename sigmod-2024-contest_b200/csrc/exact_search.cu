@@ -1020,3 +1020,102 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
 }
 
 }  // namespace fknn
+
+// ===================================================== no-allocation form
+//
+// fknn_filter_rows_noalloc: the predicate-compaction kernels above, for
+// callers that must not allocate device memory.  Their only scratch (one
+// counter per 4096-row tile plus the total) lives in the fixed array below,
+// which the module holds on every GPU that loads this library until the
+// process exits.
+
+namespace fknn {
+
+constexpr uint32_t NOALLOC_FILTER_MAX_TILES = 1u << 16;  // 65,536 tiles x 4,096 rows = 268,435,456 rows
+constexpr uint64_t NOALLOC_FILTER_MAX_ROWS = (uint64_t)NOALLOC_FILTER_MAX_TILES * FC_TILE;
+constexpr int NOALLOC_MAX_DEVICES = 64;
+
+static __device__ __align__(256) uint32_t g_noalloc_filter_scratch[NOALLOC_FILTER_MAX_TILES + 1];
+
+static std::mutex g_noalloc_mu;
+static uint32_t *g_noalloc_ptr[NOALLOC_MAX_DEVICES];
+
+// Device address of the scratch array on the current device.  The array's
+// name in host code is only a host-side handle, so the address is looked up
+// once per device (with that device current) and cached.
+static int noalloc_scratch(uint32_t **out) {
+  int dev = 0;
+  FKNN_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) {
+    set_error("fknn_filter_rows_noalloc: device ordinal above 63");
+    return FKNN_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void *p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_filter_scratch);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_noalloc_filter_scratch)");
+    g_noalloc_ptr[dev] = static_cast<uint32_t *>(p);
+  }
+  *out = g_noalloc_ptr[dev];
+  return FKNN_OK;
+}
+
+static bool on_device(const void *p) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+}
+
+}  // namespace fknn
+
+extern "C" int fknn_filter_rows_noalloc(const float *labels, const float *ts, uint64_t n, const float *meta4,
+                                        uint32_t *out_ids, uint64_t *count, void *stream) {
+  using namespace fknn;
+  g_launches = 0;
+  if (!labels || !ts || !meta4 || !out_ids || !count) {
+    set_error("fknn_filter_rows_noalloc: NULL argument");
+    return FKNN_EINVAL;
+  }
+  if (n > NOALLOC_FILTER_MAX_ROWS) {
+    set_error("fknn_filter_rows_noalloc: n = " + std::to_string(n) + " exceeds the fixed scratch limit of " +
+              std::to_string(NOALLOC_FILTER_MAX_ROWS) + " rows (65,536 tiles of 4,096)");
+    return FKNN_EINVAL;
+  }
+  const float t = meta4[0];
+  if (!(t == 0.f || t == 1.f || t == 2.f || t == 3.f)) {
+    set_error("fknn_filter_rows_noalloc: query type not in {0,1,2,3}");
+    return FKNN_EINVAL;
+  }
+  if ((t == 1.f || t == 3.f) && !(fabsf(meta4[1]) < 2147483648.f)) {
+    set_error("fknn_filter_rows_noalloc: category outside int32");
+    return FKNN_EINVAL;
+  }
+  *count = 0;
+  if (n == 0) return FKNN_OK;
+  if (!on_device(labels) || !on_device(ts) || !on_device(out_ids)) {
+    set_error("fknn_filter_rows_noalloc: labels, ts and out_ids must be device memory of the current device");
+    return FKNN_EINVAL;
+  }
+  uint32_t *tc = nullptr;
+  int rc = noalloc_scratch(&tc);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  const uint32_t ntiles = (uint32_t)((n + FC_TILE - 1) / FC_TILE);
+  const float4 m = make_float4(meta4[0], meta4[1], meta4[2], meta4[3]);
+  // every tile counter and the total are rewritten by this call, so nothing
+  // left in the array by an earlier call is read
+  k_filter_count<<<ntiles, FC_THREADS, 0, st>>>(labels, ts, n, m, tc);
+  k_exclusive_scan_small<<<1, 1, 0, st>>>(tc, ntiles, tc + ntiles);
+  k_filter_write<<<ntiles, FC_THREADS, 0, st>>>(labels, ts, n, m, tc, out_ids);
+  g_launches += 3;
+  FKNN_CUDA(cudaGetLastError());
+  uint32_t tot = 0;
+  FKNN_CUDA(cudaMemcpyAsync(&tot, tc + ntiles, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  *count = tot;
+  return FKNN_OK;
+}

@@ -84,6 +84,8 @@ SIGNATURES = {
                                c_void_p, c_void_p, POINTER(SearchStats)]),
     "fknn_count_matches": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
     "fknn_filter_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), c_void_p]),
+    "fknn_filter_rows_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, POINTER(c_uint64),
+                                         c_void_p]),
     "fknn_bruteforce_rows": (c_int, [c_void_p, c_uint32, c_void_p, c_uint32, c_void_p]),
     "fknn_sq8_sym_train": (c_int, [c_void_p, c_uint64, POINTER(c_float), c_void_p]),
     "fknn_sq8_sym_encode": (c_int, [c_void_p, c_uint64, c_float, c_void_p]),
