@@ -9,6 +9,11 @@ uniform type 0..3, k=100.  One step = one fknn_search over the whole query
 batch.  The base (two 404 MB row orders) is larger than the 126 MB L2, so
 steps are not served from cache.
 
+Both forms run on the workload: the exact FP32 path (ids bit-identical to
+the reference brute force) and the BF16 tensor-core screen + FP32 re-rank
+(k' = --kprime).  The headline is the BF16 form when its recall@100 against
+the exact path's ids over all queries is >= 0.99, else the exact path.
+
 Printed: one JSON line (rank 0).  value = queries/s with inputs resident in
 HBM; e2e = the same through the C ABI with pinned host buffers (H2D of the
 queries, D2H of ids + distances inside the timed region).  Multi-GPU runs
@@ -47,6 +52,7 @@ def parse():
     ap.add_argument("--nq", type=int, default=None, help="override queries per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="queries in the CPU-baseline sample")
+    ap.add_argument("--kprime", type=int, default=200, help="candidate width of the BF16 form")
     return ap.parse_args()
 
 
@@ -246,50 +252,66 @@ def main():
     # every rank its own query batch (weak scaling); rank 0 = the workload's queries
     q, metas = datagen.make_queries(nq, w.zipf_s, w.n_labels, w.window, w.balanced_types, 1234 + args.config,
                                     1235 + args.config + 1000 * rank)
-    idx = fknn.Index(vecs, labels, ts, device=local)
+    idx = fknn.Index(vecs, labels, ts, device=local, build_bf16=True)
     stream = torch.cuda.current_stream()
     dq = torch.from_numpy(q).cuda()
     dm = torch.from_numpy(metas).cuda()
     ids = torch.empty((nq, 100), dtype=torch.int32, device="cuda")
     dd = torch.empty((nq, 100), dtype=torch.float32, device="cuda")
 
-    def step_device():
-        return idx.search(dq, dm, k=100, ids=ids, dists=dd, stream=stream.cuda_stream, return_stats=True)[2]
-
-    for _ in range(args.warmup):
-        step_device()
-    # correctness spot check (not timed): 64 queries against the oracle
-    check = None
-    if rank == 0:
-        import oracle
-        sel = np.arange(0, nq, max(1, nq // 64))[:64]
-        oids, _ = oracle.exact_knn(vecs, labels, ts, q[sel], metas[sel])
-        check = bool(np.array_equal(ids.cpu().numpy().view(np.uint32)[sel], oids))
-
     def barrier():
         if world > 1:
             dist.barrier()
         torch.cuda.synchronize()
 
+    def max_over_ranks(x):
+        if world > 1:
+            t = torch.tensor([x], device="cuda")
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            return float(t.item())
+        return x
+
+    def timed(mode, kprime, out_ids):
+        """W untimed steps, then K steps between barriers, CUDA events on the
+        launching stream; returns (ms per step, per-step stats)."""
+        def step():
+            return idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=out_ids, dists=dd,
+                              stream=stream.cuda_stream, return_stats=True)[2]
+        for _ in range(args.warmup):
+            step()
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        st = []
+        e0.record(stream)
+        for _ in range(args.steps):
+            st.append(step())
+        e1.record(stream)
+        barrier()
+        return max_over_ranks(e0.elapsed_time(e1) / args.steps), st
+
     clocks = ClockSampler(local)
-    barrier()
     clocks.start()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    stats = []
-    e0.record(stream)
-    for _ in range(args.steps):
-        stats.append(step_device())
-    e1.record(stream)
-    barrier()
+    ms_exact, st_exact = timed(fknn.MODE_EXACT_FP32, 0, ids)
+    exact_ids = ids.cpu().numpy().view(np.uint32).copy()
+    ids_b = torch.empty_like(ids)
+    ms_bf16, st_bf16 = timed(fknn.MODE_BF16_RERANK, args.kprime, ids_b)
     clk = clocks.stop()
-    ms = e0.elapsed_time(e1) / args.steps
-    if world > 1:
-        t = torch.tensor([ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    bf16_ids = ids_b.cpu().numpy().view(np.uint32)
+    recall_bf16 = datagen.recall_matrix(bf16_ids, exact_ids)
+    use_bf16 = recall_bf16 >= 0.99
+    head_mode = fknn.MODE_BF16_RERANK if use_bf16 else fknn.MODE_EXACT_FP32
+    ms = ms_bf16 if use_bf16 else ms_exact
     value = world * nq / (ms * 1e-3)
 
-    # end to end: pinned host buffers, copies inside the timed region
+    # correctness spot check of the exact path (not timed): 64 queries vs the oracle
+    check = None
+    if rank == 0:
+        import oracle
+        sel = np.arange(0, nq, max(1, nq // 64))[:64]
+        oids, _ = oracle.exact_knn(vecs, labels, ts, q[sel], metas[sel])
+        check = bool(np.array_equal(exact_ids[sel], oids))
+
+    # end to end through the C ABI: pinned host buffers, copies inside the timed region
     hq = torch.empty((nq, 100), dtype=torch.float32, pin_memory=True).numpy()
     hm = torch.empty((nq, 4), dtype=torch.float32, pin_memory=True).numpy()
     hq[:] = q
@@ -297,57 +319,78 @@ def main():
     hids = torch.empty((nq, 100), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     hd = torch.empty((nq, 100), dtype=torch.float32, pin_memory=True).numpy()
     for _ in range(2):
-        idx.search(hq, hm, k=100, ids=hids, dists=hd, stream=stream.cuda_stream)
+        idx.search(hq, hm, k=100, mode=head_mode, kprime=args.kprime, ids=hids, dists=hd, stream=stream.cuda_stream)
     barrier()
     lat = []
     for _ in range(args.steps):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
-        idx.search(hq, hm, k=100, ids=hids, dists=hd, stream=stream.cuda_stream)
+        idx.search(hq, hm, k=100, mode=head_mode, kprime=args.kprime, ids=hids, dists=hd, stream=stream.cuda_stream)
         e.record(stream)
         e.synchronize()
         lat.append(s.elapsed_time(e))
     barrier()
-    e2e_ms = sum(lat) / len(lat)
-    if world > 1:
-        t = torch.tensor([e2e_ms], device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(sum(lat) / len(lat))
     e2e_value = world * nq / (e2e_ms * 1e-3)
-    same = bool(np.array_equal(hids, ids.cpu().numpy().view(np.uint32)))
+    same = bool(np.array_equal(hids, bf16_ids if use_bf16 else exact_ids))
 
     if rank == 0:
         peaks = measured_peaks()
         fp32_peak = fp32_gemm_peak_tflops(torch)
-        ms_screen = statistics.mean(s["ms_screen"] for s in stats)
-        pairs = stats[-1]["pairs_contraction"]
-        achieved = 2.0 * 100 * pairs / (ms_screen * 1e-3) / 1e12
         tpp = traffic_per_pair()
-        traffic = tpp * stats[-1]["pairs_screened"] if tpp else None
-        launches = int(sum(s["kernel_launches"] for s in stats))
+
+        def roof_exact():
+            ms_s = statistics.mean(x["ms_screen"] for x in st_exact)
+            pairs = st_exact[-1]["pairs_contraction"]
+            ach = 2.0 * 100 * pairs / (ms_s * 1e-3) / 1e12
+            return {"bound": "fp32_cuda_core", "kernel": "k_screen", "achieved": ach, "peak": fp32_peak,
+                    "unit": "TFLOP/s", "frac": ach / fp32_peak,
+                    "traffic": tpp * st_exact[-1]["pairs_screened"] if tpp else None,
+                    "peak_source": "cuBLAS SGEMM 8192^3 with TF32 off, measured in this run",
+                    "algorithmic": "2*d*P flops, d=100, P = passing (query,row) pairs of the contraction's queries",
+                    "per_launch_ms": ms_s, "pairs_passing": pairs, "pairs_screened": st_exact[-1]["pairs_screened"]}
+
+        def roof_bf16():
+            ms_s = statistics.mean(x["ms_screen"] for x in st_bf16)
+            pairs = st_bf16[-1]["pairs_contraction"]
+            ach = 2.0 * 100 * pairs / (ms_s * 1e-3) / 1e12
+            pk = peaks.get("bf16_tflops", 1590.0)
+            return {"bound": "tensor", "kernel": "k_screen_bf16", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk, "traffic": None,
+                    "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)" +
+                                   (" [fallback]" if peaks.get("fallback") else ""),
+                    "algorithmic": "2*d*P flops, d=100, P = passing (query,row) pairs of the contraction's queries",
+                    "per_launch_ms": ms_s, "pairs_passing": pairs, "pairs_screened": st_bf16[-1]["pairs_screened"]}
+
+        head_stats = st_bf16 if use_bf16 else st_exact
+        launches = int(sum(x["kernel_launches"] for x in head_stats))
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
-            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": w.name, "mode": "exact_fp32", "n": n, "nq_per_gpu": nq, "k": 100, "d": 100,
+            "vs_baseline": None, "dtype": "bf16" if use_bf16 else "f32", "data": "synthetic",
+            "config": {"workload": w.name, "mode": "bf16_rerank" if use_bf16 else "exact_fp32",
+                       "kprime": args.kprime if use_bf16 else None, "n": n, "nq_per_gpu": nq, "k": 100, "d": 100,
                        "parallelism": f"replicas{world}" if world > 1 else "single",
-                       "l2": "no flush: each step streams two 404 MB row orders (> 126 MB L2)"},
-            "recall_at_100_vs_exact": 1.0 if check else None, "ids_bitexact_sample64": check,
+                       "l2": "no flush: each step streams the row orders (2 x 404 MB FP32, 2 x 229 MB BF16) > 126 MB L2"},
+            "recall_at_100_vs_exact": recall_bf16 if use_bf16 else 1.0,
+            "exact_fp32": {"value": world * nq / (ms_exact * 1e-3), "ms_per_step": ms_exact,
+                           "ids_bitexact_sample64": check},
+            "bf16_rerank": {"value": world * nq / (ms_bf16 * 1e-3), "ms_per_step": ms_bf16, "kprime": args.kprime,
+                            "recall_at_100_vs_exact_all_queries": recall_bf16,
+                            "speedup_vs_exact": ms_exact / ms_bf16,
+                            "n_boundary_f64_per_step": st_bf16[-1]["n_boundary_f64"]},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nq * 100 * 4 + nq * 16),
                     "d2h_bytes_per_step": int(nq * 100 * 4 * 2), "same_ids_as_device_path": same},
             "latency_ms": {"p50": statistics.median(lat), "p99": float(np.percentile(lat, 99)),
                            "note": "per batch of nq queries, end to end"},
             "gpu_launches": launches,
-            "roofline": {"bound": "fp32_cuda_core", "kernel": "k_screen", "achieved": achieved,
-                         "peak": fp32_peak, "unit": "TFLOP/s", "frac": achieved / fp32_peak, "traffic": traffic,
-                         "peak_source": "cuBLAS SGEMM 8192^3 with TF32 off, measured in this run",
-                         "algorithmic": "2*d*P flops, P = passing (query,row) pairs of the contraction's queries",
-                         "per_launch_ms": ms_screen, "pairs_passing": pairs,
-                         "pairs_screened": stats[-1]["pairs_screened"],
-                         "hbm_peak_gbs": peaks.get("hbm_gbs")},
-            "kernel_ms": {"screen": ms_screen, "merge": statistics.mean(s["ms_merge"] for s in stats),
-                          "exact_scan": statistics.mean(s["ms_scan"] for s in stats),
-                          "plan_host": statistics.mean(s["ms_plan"] for s in stats)},
+            "roofline": roof_bf16() if use_bf16 else roof_exact(),
+            "roofline_exact_fp32": roof_exact(),
+            "kernel_ms": {m: {"screen": statistics.mean(x["ms_screen"] for x in stx),
+                              "merge": statistics.mean(x["ms_merge"] for x in stx),
+                              "exact_scan": statistics.mean(x["ms_scan"] for x in stx),
+                              "plan_host": statistics.mean(x["ms_plan"] for x in stx)}
+                          for m, stx in (("exact_fp32", st_exact), ("bf16_rerank", st_bf16))},
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu_baseline:

@@ -1,0 +1,715 @@
+// Reduced-precision form: BF16 tensor-core screen (tcgen05, FP32 accumulate
+// in TMEM) into a widened candidate list of k' per query, FP32 re-rank from
+// the original vectors with the reference's arithmetic (distance.h:62-72),
+// FP64 recompute of the candidates within 1e-6 relative of the k-th FP32
+// distance so the boundary order follows exact arithmetic.
+//
+// Layouts (both operands K-major, no swizzle, core matrices of 8 rows x 16 B):
+//   query tile A: 128 queries x 112 bf16, element (q, k) at
+//                 ((k/8)*16 + q/8)*64 + (q%8)*8 + k%8
+//   row block  B: 128 rows x 112 bf16, same formula with the row index
+// Dims 0..99 carry the vector; on the row side dims 100/101 carry
+// -|x|^2/2 split into a bf16 high part and a bf16 remainder, on the query
+// side dims 100/101 are 1.0.  The MMA therefore produces
+// acc = q.x - |x|^2/2, and ds = |q|^2 - 2*acc approximates |q - x|^2 with no
+// per-row term left for the epilogue: a row is a candidate for query q iff
+// acc >= (|q|^2 - T_q)/2, one compare per TMEM value.
+#include <algorithm>
+#include <chrono>
+#include <cstring>
+
+#include <cuda_bf16.h>
+
+#include "device_util.cuh"
+
+namespace fknn {
+
+namespace {
+
+constexpr int BQ = 128;                       // queries per tile = MMA M = TMEM lanes
+constexpr int BR = 128;                       // rows per sub-tile = MMA N
+constexpr int BK = 112;                       // padded K
+constexpr uint32_t BF_TILE = BQ * BK * 2;     // 28672 bytes, both operands
+constexpr int BS = 2;                         // shared-memory stages for row blocks
+constexpr int B_EPI_WARPS = 4;
+constexpr int B_THREADS = (2 + B_EPI_WARPS) * 32;  // producer, MMA issuer, 4 epilogue warps
+constexpr uint32_t TMEM_COLS = 2 * BR;        // double-buffered accumulator
+
+__host__ __device__ __forceinline__ uint32_t cm_index(uint32_t r, uint32_t k) {
+  return ((k >> 3) * (BQ / 8) + (r >> 3)) * 64 + (r & 7) * 8 + (k & 7);
+}
+
+// ------------------------------------------------------------ tcgen05 --
+
+__device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint32_t sbo) {
+  uint64_t d = 0;
+  d |= (uint64_t)((saddr >> 4) & 0x3FFF);
+  d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+  d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+  d |= (uint64_t)1 << 46;  // descriptor version for sm_100; base offset 0, no swizzle
+  return d;
+}
+
+// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both K-major.
+constexpr uint32_t IDESC_BF16 =
+    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BR >> 3) << 17) | ((uint32_t)(BQ >> 4) << 24);
+
+__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(IDESC_BF16), "r"(accumulate));
+}
+
+__device__ __forceinline__ void umma_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
+  uint32_t r[32];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+      "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]),
+        "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]),
+        "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+__device__ __forceinline__ void mbar_arrive1(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// ------------------------------------------------------------- build ---
+
+__global__ void k_build_bf16_blocks(const float *__restrict__ vecs, const float *__restrict__ norms,
+                                    const uint32_t *__restrict__ perm, uint64_t n, __nv_bfloat16 *__restrict__ out) {
+  const uint64_t b = blockIdx.x;
+  __nv_bfloat16 *o = out + b * (BF_TILE / 2);
+  for (uint32_t i = threadIdx.x; i < (uint32_t)BR * BK; i += blockDim.x) {
+    const uint32_t r = i / BK, k = i % BK;
+    const uint64_t p = b * BR + r;
+    float v = 0.f;
+    if (p < n) {
+      const uint32_t id = perm[p];
+      if (k < (uint32_t)DIM) {
+        v = vecs[(uint64_t)id * DIM + k];
+      } else if (k == DIM || k == DIM + 1) {
+        const float h = -0.5f * norms[id];
+        const float hi = __bfloat162float(__float2bfloat16_rn(h));
+        v = (k == DIM) ? hi : h - hi;
+      }
+    }
+    o[cm_index(r, k)] = __float2bfloat16_rn(v);
+  }
+}
+
+__global__ void k_tile_stage_bf16(const float *__restrict__ q, const int32_t *__restrict__ lane_q,
+                                  __nv_bfloat16 *__restrict__ out) {
+  const uint32_t t = blockIdx.x;
+  __nv_bfloat16 *o = out + (uint64_t)t * (BF_TILE / 2);
+  for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * BK; i += blockDim.x) {
+    const uint32_t l = i / BK, k = i % BK;
+    const int32_t qi = lane_q[t * BQ + l];
+    float v = 0.f;
+    if (qi >= 0) {
+      if (k < (uint32_t)DIM) v = q[(uint64_t)qi * DIM + k];
+      else if (k == DIM || k == DIM + 1) v = 1.f;
+    }
+    o[cm_index(l, k)] = __float2bfloat16_rn(v);
+  }
+}
+
+// ------------------------------------------------------------ screen ---
+
+struct BScreenSmem {
+  unsigned char a[BF_TILE];
+  unsigned char b[BS][BF_TILE];
+  float thr[BQ];  // current k'-th screening distance bound T
+  float qn[BQ];
+  int cnt[BQ];
+  int32_t lq[BQ];
+  uint32_t hist[B_EPI_WARPS][256];
+  uint64_t full[BS], empty[BS], accfull[2], accempty[2], abar;
+  uint32_t tmem_base;
+};
+
+// kth smallest screening distance of a list (warp radix select over the
+// order-preserving integer image; 4 passes of 8 bits).
+__device__ float warp_select_kth(const Candidate *list, int n, int kth, uint32_t *hist) {
+  const int lane = threadIdx.x & 31;
+  uint32_t prefix = 0, mask = 0;
+  int remaining = kth;
+  for (int pass = 0; pass < 4; ++pass) {
+    const int shift = 24 - 8 * pass;
+    for (int i = lane; i < 256; i += 32) hist[i] = 0;
+    __syncwarp();
+    for (int i = lane; i < n; i += 32) {
+      const uint32_t u = f32_sortable(list[i].ds);
+      if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255], 1u);
+    }
+    __syncwarp();
+    uint32_t local[8], s = 0;
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      local[j] = hist[lane * 8 + j];
+      s += local[j];
+    }
+    uint32_t inc = s;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    const uint32_t excl = inc - s;
+    const uint32_t hit = __ballot_sync(0xffffffffu, excl < (uint32_t)remaining && inc >= (uint32_t)remaining);
+    const int owner = __ffs(hit) - 1;
+    uint32_t bin = 0, before = 0;
+    if (lane == owner) {
+      uint32_t c = excl;
+      for (int j = 0; j < 8; ++j) {
+        if (c + local[j] >= (uint32_t)remaining) {
+          bin = lane * 8 + j;
+          before = c;
+          break;
+        }
+        c += local[j];
+      }
+    }
+    bin = __shfl_sync(0xffffffffu, bin, owner);
+    before = __shfl_sync(0xffffffffu, before, owner);
+    remaining -= (int)before;
+    prefix |= bin << shift;
+    mask |= 255u << shift;
+    __syncwarp();
+  }
+  return sortable_f32(prefix);
+}
+
+// Bound and trim list L to its k' smallest screening distances (ties kept).
+__device__ __noinline__ void bcompact(Candidate *list, BScreenSmem &sm, int L, int wslot, uint32_t kprime,
+                                      uint32_t capb, uint32_t *T_global, uint32_t *ovf) {
+  const int lane = threadIdx.x & 31;
+  const int n = sm.cnt[L];
+  const int32_t qi = sm.lq[L];
+  float T = sm.thr[L];
+  if (n >= (int)kprime) T = fminf(T, warp_select_kth(list, n, (int)kprime, sm.hist[wslot]));
+  const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+  if (Tg < T) T = Tg;
+  if (lane == 0 && T < Tg) atomicMin(T_global + qi, f32_sortable(T));
+  // in-place stable compaction of the entries with ds <= T
+  int kept = 0;
+  const uint32_t lt = (1u << lane) - 1u;
+  for (int base = 0; base < n; base += 32) {
+    const int i = base + lane;
+    Candidate c;
+    bool keep = false;
+    if (i < n) {
+      c = list[i];
+      keep = c.ds <= T;
+    }
+    const uint32_t b = __ballot_sync(0xffffffffu, keep);
+    __syncwarp();
+    if (keep) list[kept + __popc(b & lt)] = c;
+    kept += __popc(b);
+    __syncwarp();
+  }
+  if (lane == 0) {
+    if (kept > (int)capb - BR) {
+      ovf[qi] = 1u;  // a tie flood: the exact scan answers this query
+      sm.cnt[L] = 0;
+      sm.thr[L] = -INFINITY;
+    } else {
+      sm.cnt[L] = kept;
+      sm.thr[L] = T;
+    }
+  }
+  __syncwarp();
+}
+
+__global__ void __launch_bounds__(B_THREADS, 2)
+    k_screen_bf16(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles,
+                  const unsigned char *__restrict__ atiles, const int32_t *__restrict__ lane_q,
+                  const uint32_t *__restrict__ lane_s, const uint32_t *__restrict__ lane_e,
+                  const QueryDesc *__restrict__ desc, const unsigned char *__restrict__ blocks_t,
+                  const unsigned char *__restrict__ blocks_c, uint32_t *__restrict__ T_global,
+                  uint32_t *__restrict__ ovf, Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt,
+                  uint32_t kprime, uint32_t capb, int *err) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  BScreenSmem &sm = *reinterpret_cast<BScreenSmem *>(smem_raw);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t item_id = blockIdx.x;
+  const WorkItem it = items[item_id];
+  const Tile tl = tiles[it.tile];
+  const unsigned char *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
+  const uint32_t nsub = it.blk1 - it.blk0;
+
+  if (tid == 0) {
+    for (int s = 0; s < BS; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sm.accfull[a], 1);
+      mbar_init(&sm.accempty[a], B_EPI_WARPS);
+    }
+    mbar_init(&sm.abar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
+                 "r"(TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (warp == 0) {
+    // ------------------------------------------------ producer
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&sm.abar, BF_TILE);
+      bulk_g2s(sm.a, atiles + (uint64_t)it.tile * BF_TILE, BF_TILE, &sm.abar);
+      uint32_t issued = 0;
+      for (uint32_t sub = 0; sub < nsub; ++sub) {
+        const int st = sub % BS;
+        if (sub >= BS && !mbar_wait_bounded(&sm.empty[st], ((sub / BS) - 1) & 1, err)) break;
+        mbar_arrive_expect_tx(&sm.full[st], BF_TILE);
+        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub) * BF_TILE, BF_TILE, &sm.full[st]);
+        ++issued;
+      }
+      mbar_wait_bounded(&sm.abar, 0, err);
+      for (uint32_t i = issued > BS ? issued - BS : 0; i < issued; ++i)
+        mbar_wait_bounded(&sm.full[i % BS], (i / BS) & 1, err);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      uint32_t done = 0;
+      if (mbar_wait_bounded(&sm.abar, 0, err)) {
+        const uint32_t a0 = smem_u32(sm.a);
+        for (uint32_t sub = 0; sub < nsub; ++sub) {
+          const int st = sub % BS, ab = sub & 1;
+          if (!mbar_wait_bounded(&sm.full[st], (sub / BS) & 1, err)) break;
+          if (sub >= 2 && !mbar_wait_bounded(&sm.accempty[ab], ((sub >> 1) - 1) & 1, err)) break;
+          tc_fence_after();
+          const uint32_t b0 = smem_u32(sm.b[st]);
+#pragma unroll
+          for (int kk = 0; kk < BK / 16; ++kk) {
+            const uint64_t da = umma_desc(a0 + kk * 2 * (BQ / 8) * 128, (BQ / 8) * 128, 128);
+            const uint64_t db = umma_desc(b0 + kk * 2 * (BR / 8) * 128, (BR / 8) * 128, 128);
+            umma_bf16(tmem + ab * BR, da, db, kk > 0);
+          }
+          umma_commit(&sm.empty[st]);     // the row block may be overwritten once these MMAs finish
+          umma_commit(&sm.accfull[ab]);   // the accumulator is ready for the epilogue
+          ++done;
+        }
+      }
+      // no MMA may be in flight when TMEM is released
+      if (done) mbar_wait_bounded(&sm.accfull[(done - 1) & 1], ((done - 1) >> 1) & 1, err);
+    }
+  } else {
+    // ------------------------------------------------ epilogue: thread = query
+    const int wslot = warp - 2;
+    const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
+    const int L = wg * 32 + lane;
+    const int32_t qi = lane_q[it.tile * BQ + L];
+    float qn = 0.f;
+    uint32_t s = 0, e = 0;
+    float T = -INFINITY;
+    if (qi >= 0) {
+      qn = desc[qi].qn;
+      s = lane_s[it.tile * BQ + L];
+      e = lane_e[it.tile * BQ + L];
+      T = sortable_f32(ld_volatile_u32(T_global + qi));
+      if (ld_volatile_u32(ovf + qi)) T = -INFINITY;
+    }
+    sm.lq[L] = qi;
+    sm.cnt[L] = 0;
+    sm.thr[L] = T;
+    __syncwarp();
+    Candidate *list = out + ((uint64_t)item_id * BQ + L) * capb;
+    int cnt = 0;
+    bool ok = true;
+    for (uint32_t sub = 0; sub < nsub; ++sub) {
+      const int ab = sub & 1;
+      if (!mbar_wait_bounded(&sm.accfull[ab], (sub >> 1) & 1, err)) {
+        ok = false;
+        break;
+      }
+      tc_fence_after();
+      const uint32_t p0 = (it.blk0 + sub) * BR;
+      const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
+      const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
+      // candidate iff qn - 2*acc <= T  <=>  acc >= (qn - T) / 2
+      const float cq = (T == INFINITY) ? -INFINITY : 0.5f * (qn - T);
+#pragma unroll 1
+      for (int c = 0; c < BR; c += 32) {
+        float v[32];
+        tmem_ld32(tmem + ((uint32_t)(wg * 32) << 16) + ab * BR + c, v);
+        if (r0 >= c + 32 || r1 <= c) continue;
+        float m = -INFINITY;
+        const bool whole = r0 <= c && r1 >= c + 32;
+        if (whole) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) m = fmaxf(m, v[j]);
+        } else {
+#pragma unroll
+          for (int j = 0; j < 32; ++j)
+            if (c + j >= r0 && c + j < r1) m = fmaxf(m, v[j]);
+        }
+        if (m >= cq) {
+#pragma unroll
+          for (int j = 0; j < 32; ++j) {
+            if (v[j] >= cq && c + j >= r0 && c + j < r1) {
+              Candidate cd;
+              cd.ds = fmaf(-2.f, v[j], qn);
+              cd.pos = p0 + c + j;
+              list[cnt++] = cd;
+            }
+          }
+        }
+      }
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&sm.accempty[ab]);
+      // lists that could overflow in the next sub-tile are bounded and trimmed
+      sm.cnt[L] = cnt;
+      const bool need = cnt > (int)capb - BR;
+      uint32_t msk = __ballot_sync(0xffffffffu, need);
+      __syncwarp();
+      while (msk) {
+        const int b = __ffs(msk) - 1;
+        msk &= msk - 1;
+        const int Lb = wg * 32 + b;
+        bcompact(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+      }
+      cnt = sm.cnt[L];
+      T = sm.thr[L];
+    }
+    if (!ok) {
+      if (qi >= 0) ovf[qi] = 1u;
+      out_cnt[(uint64_t)item_id * BQ + L] = 0;
+    } else {
+      sm.cnt[L] = cnt;
+      __syncwarp();
+      for (int b = 0; b < 32; ++b) {
+        const int Lb = wg * 32 + b;
+        if (sm.cnt[Lb] > 0 && sm.lq[Lb] >= 0)
+          bcompact(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+      }
+      out_cnt[(uint64_t)item_id * BQ + L] = (uint32_t)sm.cnt[L];
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
+  }
+}
+
+// ------------------------------------------------------------ re-rank --
+
+constexpr int RR_THREADS = 256;
+constexpr int RR_CAP = 8192;  // screening candidates one block can hold
+constexpr int RR_KMAX = 1024; // largest k'
+
+struct RerankSmem {
+  float key[RR_CAP];
+  uint32_t val[RR_CAP];
+  uint64_t ekey[RR_KMAX];
+  float qv[DIM];
+  uint32_t cnt_prefix[RR_THREADS + 1];
+  int total;
+};
+
+__global__ void __launch_bounds__(RR_THREADS)
+    k_merge_rerank(const uint32_t *__restrict__ big_q, const uint32_t *__restrict__ big_tile,
+                   const uint32_t *__restrict__ big_lane, const Tile *__restrict__ tiles,
+                   const uint32_t *__restrict__ item_slot, const Candidate *__restrict__ out,
+                   const uint32_t *__restrict__ out_cnt, const QueryDesc *__restrict__ desc,
+                   const float *__restrict__ q, const float *__restrict__ vecs, const uint32_t *__restrict__ perm_t,
+                   const uint32_t *__restrict__ perm_c, const uint32_t *__restrict__ ovf,
+                   uint32_t *__restrict__ ovf_list, uint32_t *__restrict__ ovf_count, uint32_t k, uint32_t kprime,
+                   uint32_t capb, uint32_t *__restrict__ ids, float *__restrict__ dists,
+                   uint32_t *__restrict__ n_f64) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  RerankSmem &sm = *reinterpret_cast<RerankSmem *>(smem_raw);
+  const int tid = threadIdx.x;
+  const uint32_t qi = big_q[blockIdx.x];
+  if (ovf[qi]) {
+    if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
+    return;
+  }
+  const Tile tl = tiles[big_tile[blockIdx.x]];
+  const uint32_t L = big_lane[blockIdx.x];
+  const uint32_t nitems = tl.item1 - tl.item0;
+  const QueryDesc dsc = desc[qi];
+  for (int d = tid; d < DIM; d += RR_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
+  const uint32_t per = (nitems + RR_THREADS - 1) / RR_THREADS;
+  const uint32_t ib = tid * per, ie = min(ib + per, nitems);
+  uint32_t mine = 0;
+  for (uint32_t i = ib; i < ie; ++i) mine += out_cnt[(uint64_t)item_slot[tl.item0 + i] * BQ + L];
+  sm.cnt_prefix[tid + 1] = mine;
+  if (tid == 0) sm.cnt_prefix[0] = 0;
+  __syncthreads();
+  if (tid == 0) {
+    for (int t = 0; t < RR_THREADS; ++t) sm.cnt_prefix[t + 1] += sm.cnt_prefix[t];
+    sm.total = (int)sm.cnt_prefix[RR_THREADS];
+  }
+  __syncthreads();
+  const int M = sm.total;
+  if (M > RR_CAP) {
+    if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
+    return;
+  }
+  {
+    uint32_t w = sm.cnt_prefix[tid];
+    for (uint32_t i = ib; i < ie; ++i) {
+      const uint64_t item = item_slot[tl.item0 + i];
+      const uint32_t c = out_cnt[item * BQ + L];
+      const Candidate *src = out + (item * BQ + L) * capb;
+      for (uint32_t j = 0; j < c; ++j) {
+        const Candidate cd = src[j];
+        sm.key[w] = cd.ds;
+        sm.val[w] = cd.pos;
+        ++w;
+      }
+    }
+  }
+  int np2 = 32;
+  while (np2 < M) np2 <<= 1;
+  for (int i = M + tid; i < np2; i += RR_THREADS) {
+    sm.key[i] = INFINITY;
+    sm.val[i] = 0xffffffffu;
+  }
+  __syncthreads();
+  block_bitonic_sort_kv(sm.key, sm.val, np2);
+  // FP32 re-rank of the k' best screened rows with the reference's arithmetic
+  const int C = min(M, (int)kprime);
+  const uint32_t *perm = dsc.order == ORDER_TIME ? perm_t : perm_c;
+  for (int i = tid; i < C; i += RR_THREADS) {
+    const uint32_t id = perm[sm.val[i]];
+    const float d = seq_l2_strided(vecs + (uint64_t)id * DIM, 1, sm.qv);
+    sm.ekey[i] = exact_key(d, id);
+  }
+  int cp2 = 32;
+  while (cp2 < C) cp2 <<= 1;
+  for (int i = C + tid; i < cp2; i += RR_THREADS) sm.ekey[i] = ~0ull;
+  __syncthreads();
+  block_bitonic_sort(sm.ekey, cp2);
+  // FP64 at the k-th boundary: candidates within 1e-6 relative of the k-th
+  // FP32 distance are ordered by their exact double distance
+  if (tid == 0 && C > 0) {
+    const int kk = min((int)k, C);
+    const float D = sortable_f32((uint32_t)(sm.ekey[kk - 1] >> 32));
+    const float lo = D - 1e-6f * D, hi = D + 1e-6f * D;
+    int i0 = kk - 1, i1 = kk;
+    while (i0 > 0 && sortable_f32((uint32_t)(sm.ekey[i0 - 1] >> 32)) >= lo) --i0;
+    while (i1 < C && sortable_f32((uint32_t)(sm.ekey[i1] >> 32)) <= hi) ++i1;
+    if (i1 - i0 > 1) {
+      double d64[64];
+      const int nb = min(i1 - i0, 64);
+      for (int j = 0; j < nb; ++j) {
+        const uint32_t id = (uint32_t)sm.ekey[i0 + j];
+        const float *x = vecs + (uint64_t)id * DIM;
+        double s = 0.0;
+        for (int d = 0; d < DIM; ++d) {
+          const double t = (double)x[d] - (double)sm.qv[d];
+          s += t * t;
+        }
+        d64[j] = s;
+      }
+      for (int a = 1; a < nb; ++a) {  // insertion sort by (d64, id)
+        const double dv = d64[a];
+        const uint64_t kv = sm.ekey[i0 + a];
+        int b = a - 1;
+        while (b >= 0 && (d64[b] > dv || (d64[b] == dv && (uint32_t)sm.ekey[i0 + b] > (uint32_t)kv))) {
+          d64[b + 1] = d64[b];
+          sm.ekey[i0 + b + 1] = sm.ekey[i0 + b];
+          --b;
+        }
+        d64[b + 1] = dv;
+        sm.ekey[i0 + b + 1] = kv;
+      }
+      atomicAdd(n_f64, (uint32_t)nb);
+    }
+  }
+  __syncthreads();
+  for (uint32_t j = tid; j < k; j += RR_THREADS) {
+    uint32_t id = 0xffffffffu;
+    float d = INFINITY;
+    if ((int)j < C) {
+      id = (uint32_t)sm.ekey[j];
+      d = sortable_f32((uint32_t)(sm.ekey[j] >> 32));
+    }
+    ids[(uint64_t)qi * k + j] = id;
+    if (dists) dists[(uint64_t)qi * k + j] = d;
+  }
+}
+
+inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
+
+}  // namespace
+
+int build_bf16(fknn_index *idx, cudaStream_t st) {
+  const uint64_t nblk = (idx->n + BR - 1) / BR;
+  for (int o = 0; o < 2; ++o) {
+    int rc = dev_alloc(idx, &idx->bf16_blocks[o], nblk * BF_TILE);
+    if (rc) return rc;
+    k_build_bf16_blocks<<<(unsigned)nblk, 256, 0, st>>>(idx->vecs, idx->norms, idx->ord[o].perm, idx->n,
+                                                        (__nv_bfloat16 *)idx->bf16_blocks[o]);
+    g_launches += 1;
+  }
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+                uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  const uint64_t n = idx->n;
+  int rc;
+  QueryDesc *d_desc, *h_desc;
+  float *h_meta;
+  if ((rc = prepare_queries(idx, d_q, d_meta, nq, st, &d_desc, &h_desc, &h_meta))) return rc;
+  // candidate slots per (item, query): k' plus one sub-tile of pushes plus slack
+  const uint32_t capb = (uint32_t)align_up(kprime + 2 * BR, 128);
+  auto t0 = std::chrono::steady_clock::now();
+  Plan P;
+  PlanShape shape;
+  shape.tq = BQ;
+  shape.blk_rows = BR;
+  shape.small_slab = SMALL_SLAB;
+  // candidate scratch (items x 128 x capb x 8 B) stays within ~8 GB
+  const uint64_t per_item = (uint64_t)BQ * capb * sizeof(Candidate);
+  const uint64_t tiles_est = std::max<uint64_t>(1, (nq + BQ - 1) / BQ);
+  shape.max_items_per_tile = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>(RR_CAP / capb, (8ull << 30) / (per_item * tiles_est)));
+  shape.min_chunk_blocks = 8;
+  shape.target_items = 148 * 2 * 3;
+  make_plan(h_desc, h_meta, nq, n, shape, P);
+  auto t1 = std::chrono::steady_clock::now();
+  const uint32_t ntile = (uint32_t)P.tiles.size(), nitems = (uint32_t)P.items.size();
+  const uint32_t nbig = (uint32_t)P.big.size(), nsmall = (uint32_t)P.small.size();
+  std::vector<uint32_t> slot(nitems);
+  {
+    std::vector<uint32_t> fill(ntile);
+    for (uint32_t t = 0; t < ntile; ++t) fill[t] = P.tiles[t].item0;
+    for (uint32_t s = 0; s < nitems; ++s) slot[fill[P.items[s].tile]++] = s;
+  }
+  size_t off = 0;
+  auto take = [&](size_t bytes) {
+    size_t o = off;
+    off = align_up(off + bytes, 256);
+    return o;
+  };
+  const size_t o_small = take(nsmall * 4), o_big = take(nbig * 4), o_btile = take(nbig * 4),
+               o_blane = take(nbig * 4), o_tiles = take(ntile * sizeof(Tile)),
+               o_items = take(nitems * sizeof(WorkItem)), o_lq = take((size_t)ntile * BQ * 4),
+               o_ls = take((size_t)ntile * BQ * 4), o_le = take((size_t)ntile * BQ * 4), o_slot = take(nitems * 4);
+  const size_t blob = off;
+  unsigned char *h_blob, *d_blob;
+  if ((rc = hs_get(idx, 3, blob + 256, (void **)&h_blob))) return rc;
+  if ((rc = ws_get(idx, 3, blob + 256, (void **)&d_blob))) return rc;
+  auto put = [&](size_t o, const void *src, size_t bytes) {
+    if (bytes) std::memcpy(h_blob + o, src, bytes);
+  };
+  put(o_small, P.small.data(), nsmall * 4);
+  put(o_big, P.big.data(), nbig * 4);
+  put(o_btile, P.big_tile.data(), nbig * 4);
+  put(o_blane, P.big_lane.data(), nbig * 4);
+  put(o_tiles, P.tiles.data(), ntile * sizeof(Tile));
+  put(o_items, P.items.data(), nitems * sizeof(WorkItem));
+  put(o_lq, P.lane_q.data(), (size_t)ntile * BQ * 4);
+  put(o_ls, P.lane_s.data(), (size_t)ntile * BQ * 4);
+  put(o_le, P.lane_e.data(), (size_t)ntile * BQ * 4);
+  put(o_slot, slot.data(), nitems * 4);
+  if (blob) FKNN_CUDA(cudaMemcpyAsync(d_blob, h_blob, blob, cudaMemcpyHostToDevice, st));
+  uint32_t *d_state;
+  if ((rc = ws_get(idx, 5, (size_t)nq * 12 + 64, (void **)&d_state))) return rc;
+  uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
+           *ovf_count = d_state + 3 * (size_t)nq, *n_f64 = ovf_count + 1;
+  if ((rc = launch_fill_u32(T_global, nq, f32_sortable(INFINITY), st))) return rc;
+  FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
+  FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 8, st));
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  if (stats)
+    for (auto &e : ev) FKNN_CUDA(cudaEventCreate(&e));
+  const OrderData &OT = idx->ord[ORDER_TIME], &OC = idx->ord[ORDER_CAT];
+  if (nitems) {
+    unsigned char *d_at;
+    Candidate *d_out;
+    uint32_t *d_ocnt;
+    if ((rc = ws_get(idx, 4, (size_t)ntile * BF_TILE, (void **)&d_at))) return rc;
+    if ((rc = ws_get(idx, 6, (size_t)nitems * BQ * capb * sizeof(Candidate), (void **)&d_out))) return rc;
+    if ((rc = ws_get(idx, 7, (size_t)nitems * BQ * 4, (void **)&d_ocnt))) return rc;
+    k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), (__nv_bfloat16 *)d_at);
+    static bool attr = false;
+    if (!attr) {
+      FKNN_CUDA(cudaFuncSetAttribute(k_screen_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(BScreenSmem)));
+      FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(RerankSmem)));
+      attr = true;
+    }
+    if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
+    k_screen_bf16<<<nitems, B_THREADS, sizeof(BScreenSmem), st>>>(
+        (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
+        (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_desc,
+        (const unsigned char *)idx->bf16_blocks[ORDER_TIME], (const unsigned char *)idx->bf16_blocks[ORDER_CAT],
+        T_global, ovf, d_out, d_ocnt, kprime, capb, idx->d_flag);
+    if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
+    k_merge_rerank<<<nbig, RR_THREADS, sizeof(RerankSmem), st>>>(
+        (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
+        (const Tile *)(d_blob + o_tiles), (const uint32_t *)(d_blob + o_slot), d_out, d_ocnt, d_desc, d_q, idx->vecs,
+        OT.perm, OC.perm, ovf, ovf_list, ovf_count, k, kprime, capb, d_ids, d_dists, n_f64);
+    g_launches += 3;
+  }
+  if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));
+  if (nsmall)
+    if ((rc = launch_exact_scan(idx, (const uint32_t *)(d_blob + o_small), nullptr, nsmall,
+                                std::min<uint32_t>(nsmall, 148 * 8), d_desc, d_q, k, d_ids, d_dists, st)))
+      return rc;
+  if (nbig)
+    if ((rc = launch_exact_scan(idx, ovf_list, ovf_count, 0, 148 * 2, d_desc, d_q, k, d_ids, d_dists, st))) return rc;
+  FKNN_CUDA(cudaGetLastError());
+  if (stats) {
+    FKNN_CUDA(cudaEventRecord(ev[3], st));
+    FKNN_CUDA(cudaEventSynchronize(ev[3]));
+    float ms = 0.f;
+    if (nitems) {
+      FKNN_CUDA(cudaEventElapsedTime(&ms, ev[0], ev[1]));
+      stats->ms_screen = ms;
+      FKNN_CUDA(cudaEventElapsedTime(&ms, ev[1], ev[2]));
+      stats->ms_merge = ms;
+    }
+    FKNN_CUDA(cudaEventElapsedTime(&ms, ev[2], ev[3]));
+    stats->ms_scan = ms;
+    for (auto &e : ev) cudaEventDestroy(e);
+    stats->pairs_screened = P.pairs_screened;
+    stats->pairs_passing = P.pairs_passing;
+    stats->pairs_contraction = P.pairs_contraction;
+    stats->n_tiles = ntile;
+    stats->n_work_items = nitems;
+    stats->n_small = nsmall;
+    stats->ms_plan = std::chrono::duration<float, std::milli>(t1 - t0).count();
+    uint32_t h2[2] = {0, 0};
+    FKNN_CUDA(cudaMemcpyAsync(h2, ovf_count, 8, cudaMemcpyDeviceToHost, st));
+    FKNN_CUDA(cudaStreamSynchronize(st));
+    stats->n_overflow = h2[0];
+    stats->n_boundary_f64 = h2[1];
+  }
+  return FKNN_OK;
+}
+
+}  // namespace fknn

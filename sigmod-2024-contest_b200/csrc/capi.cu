@@ -169,8 +169,15 @@ int fknn_index_create(const float *vecs, const float *labels, const float *ts, u
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc");
   }
   if (!rc) rc = build_index(idx, vecs, labels, ts, idx->own_stream);
-  if (!rc && opts && (opts->build_bf16 || opts->build_fp8)) {
-    set_error("fknn_index_create: reduced-precision copies are not available in this build");
+  if (!rc && opts && opts->build_bf16) {
+    rc = build_bf16(idx, idx->own_stream);
+    if (!rc) {
+      cudaError_t e2 = cudaStreamSynchronize(idx->own_stream);
+      if (e2 != cudaSuccess) rc = cuda_fail(e2, "build_bf16");
+    }
+  }
+  if (!rc && opts && opts->build_fp8) {
+    set_error("fknn_index_create: FP8 codes are not available in this build");
     rc = FKNN_EUNSUPPORTED;
   }
   // build temporaries are not needed by searches
@@ -220,7 +227,17 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     set_error("fknn_search: NULL qvecs/metas/ids");
     return FKNN_EINVAL;
   }
-  if (mode != FKNN_MODE_EXACT_FP32) {
+  const uint32_t kprime = (opts && opts->kprime) ? opts->kprime : 400;
+  if (mode == FKNN_MODE_BF16_RERANK) {
+    if (!idx->bf16_blocks[0]) {
+      set_error("fknn_search: BF16 mode needs an index created with build_bf16");
+      return FKNN_EUNSUPPORTED;
+    }
+    if (kprime < k || kprime > 1024) {
+      set_error("fknn_search: kprime must be in [k, 1024]");
+      return FKNN_EINVAL;
+    }
+  } else if (mode != FKNN_MODE_EXACT_FP32) {
     set_error("fknn_search: mode not built into this index");
     return FKNN_EUNSUPPORTED;
   }
@@ -245,7 +262,8 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     if ((rc = ws_get(idx, 8, (size_t)nq * k * 4, (void **)&d_ids))) return rc;
   if (dists && !dd_dev)
     if ((rc = ws_get(idx, 9, (size_t)nq * k * 4, (void **)&d_dists))) return rc;
-  rc = search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
+  rc = mode == FKNN_MODE_BF16_RERANK ? search_bf16(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats)
+                                     : search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
   if (rc) return rc;
   if (!i_dev) FKNN_CUDA(cudaMemcpyAsync(ids, d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && !dd_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_dists, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));

@@ -163,10 +163,17 @@ __global__ void k_tile_stage(const float *__restrict__ q, const QueryDesc *__res
 
 // -------------------------------------------------------------- screen --
 
-constexpr int SC_THREADS = 128;
+constexpr int SC_CONSUMERS = 4;                   // compute warps
+constexpr int SC_THREADS = (SC_CONSUMERS + 1) * 32;  // + one producer warp
 constexpr int SC_STAGES = 3;
 constexpr int SC_REFRESH = 16;  // sub-tiles between reads of the shared bound
 
+// Each consumer warp w owns the candidate lists of queries [16w, 16w+16) of
+// the tile: with the thread mapping below (rows ty*4.., queries tx*8..,
+// tx = tid/16) only warp w ever pushes into them, so lists are compacted by
+// their owner with no CTA-wide barrier.  Row blocks stream through a ring of
+// SC_STAGES buffers: the producer warp issues one bulk copy per 64-row block
+// after the four consumer warps released the slot (empty barrier).
 struct ScreenSmem {
   float qs[BLK_FLOATS];
   float xs[SC_STAGES][BLK_FLOATS];
@@ -176,12 +183,16 @@ struct ScreenSmem {
   int cnt[TQ];
   uint32_t ls[TQ], le[TQ];
   int32_t lq[TQ];
-  uint64_t bar[SC_STAGES + 1];
+  uint64_t full[SC_STAGES], empty[SC_STAGES], qbar;
 };
 
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
 // Sort, bound and trim one (item, query) candidate list.  Whole warp.
-__device__ void compact_list(Candidate *list, ScreenSmem &sm, int L, uint32_t k, uint32_t *T_global,
-                             uint32_t *ovf) {
+__device__ __noinline__ void compact_list(Candidate *list, ScreenSmem &sm, int L, uint32_t k, uint32_t *T_global,
+                                          uint32_t *ovf) {
   const int lane = threadIdx.x & 31;
   const int n = sm.cnt[L];
   float key[CAP / 32];
@@ -262,45 +273,64 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
   Candidate *out_item = out + (uint64_t)item_id * TQ * CAP;
 
   if (tid == 0) {
-    for (int s = 0; s < SC_STAGES + 1; ++s) mbar_init(&sm.bar[s], 1);
+    for (int s = 0; s < SC_STAGES; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], SC_CONSUMERS);
+    }
+    mbar_init(&sm.qbar, 1);
     fence_mbar_init();
   }
-  __syncthreads();
-  if (tid == 0) {
-    mbar_arrive_expect_tx(&sm.bar[SC_STAGES], BLK_BYTES);
-    bulk_g2s(sm.qs, qtiles + (uint64_t)it.tile * BLK_FLOATS, BLK_BYTES, &sm.bar[SC_STAGES]);
-    for (uint32_t s = 0; s < SC_STAGES && s < nsub; ++s) {
-      mbar_arrive_expect_tx(&sm.bar[s], BLK_BYTES);
-      bulk_g2s(sm.xs[s], blocks + (uint64_t)(it.blk0 + s) * BLK_FLOATS, BLK_BYTES, &sm.bar[s]);
+  __syncthreads();  // the only CTA-wide barrier
+
+  if (warp == SC_CONSUMERS) {
+    // ---------------- producer: one lane issues every bulk copy
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&sm.qbar, BLK_BYTES);
+      bulk_g2s(sm.qs, qtiles + (uint64_t)it.tile * BLK_FLOATS, BLK_BYTES, &sm.qbar);
+      uint32_t issued = 0;
+      for (uint32_t sub = 0; sub < nsub; ++sub) {
+        const int st = sub % SC_STAGES;
+        if (sub >= SC_STAGES && !mbar_wait_bounded(&sm.empty[st], ((sub / SC_STAGES) - 1) & 1, err)) break;
+        mbar_arrive_expect_tx(&sm.full[st], BLK_BYTES);
+        bulk_g2s(sm.xs[st], blocks + (uint64_t)(it.blk0 + sub) * BLK_FLOATS, BLK_BYTES, &sm.full[st]);
+        ++issued;
+      }
+      // every issued copy must have landed before the CTA may exit
+      mbar_wait_bounded(&sm.qbar, 0, err);
+      for (uint32_t i = issued > SC_STAGES ? issued - SC_STAGES : 0; i < issued; ++i)
+        mbar_wait_bounded(&sm.full[i % SC_STAGES], (i / SC_STAGES) & 1, err);
     }
+    return;
   }
-  // every wait's outcome is made block-uniform before any barrier depends on it
-  bool ok = __syncthreads_and(mbar_wait_bounded(&sm.bar[SC_STAGES], 0, err)) != 0;
-  if (tid < TQ) {
-    const int32_t qi = lane_q[it.tile * TQ + tid];
-    sm.lq[tid] = qi;
-    sm.cnt[tid] = 0;
-    sm.qn[tid] = sm.qs[DIM * TQ + tid];
+
+  // ---------------- consumers
+  bool ok = mbar_wait_bounded(&sm.qbar, 0, err);
+  if (lane < 16) {
+    const int L = 16 * warp + lane;
+    const int32_t qi = lane_q[it.tile * TQ + L];
+    sm.lq[L] = qi;
+    sm.cnt[L] = 0;
+    sm.qn[L] = sm.qs[DIM * TQ + L];
     if (qi >= 0) {
-      sm.ls[tid] = lane_s[it.tile * TQ + tid];
-      sm.le[tid] = lane_e[it.tile * TQ + tid];
+      sm.ls[L] = lane_s[it.tile * TQ + L];
+      sm.le[L] = lane_e[it.tile * TQ + L];
       const float T = sortable_f32(ld_volatile_u32(T_global + qi));
-      sm.thr[tid] = T;
-      sm.push[tid] = (T == INFINITY) ? INFINITY : screen_push_limit(T, sm.qn[tid]);
-      if (ld_volatile_u32(ovf + qi)) sm.push[tid] = -INFINITY;
+      sm.thr[L] = T;
+      sm.push[L] = (T == INFINITY) ? INFINITY : screen_push_limit(T, sm.qn[L]);
+      if (ld_volatile_u32(ovf + qi)) sm.push[L] = -INFINITY;
     } else {
-      sm.ls[tid] = sm.le[tid] = 0;
-      sm.thr[tid] = -INFINITY;
-      sm.push[tid] = -INFINITY;
+      sm.ls[L] = sm.le[L] = 0;
+      sm.thr[L] = -INFINITY;
+      sm.push[L] = -INFINITY;
     }
   }
-  __syncthreads();
+  __syncwarp();
 
   const int ty = tid & 15;  // rows ty*4 .. ty*4+3 of the 64-row block
-  const int tx = tid >> 4;  // queries tx*8 .. tx*8+7 of the tile
+  const int tx = tid >> 4;  // queries tx*8 .. tx*8+7 of the tile (owned by this warp)
   for (uint32_t sub = 0; sub < nsub && ok; ++sub) {
     const int st = sub % SC_STAGES;
-    if (!__syncthreads_and(mbar_wait_bounded(&sm.bar[st], (sub / SC_STAGES) & 1, err))) {
+    if (!mbar_wait_bounded(&sm.full[st], (sub / SC_STAGES) & 1, err)) {
       ok = false;
       break;
     }
@@ -312,7 +342,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
       for (int j = 0; j < 8; ++j) acc[i][j] = 0.f;
     const float4 *xr = reinterpret_cast<const float4 *>(xs) + ty;
     const float4 *qr = reinterpret_cast<const float4 *>(sm.qs) + tx * 2;
-#pragma unroll 20
+#pragma unroll 10
     for (int d = 0; d < DIM; ++d) {
       const float4 a = xr[d * (BLK / 4)];
       const float4 b0 = qr[d * (TQ / 4)];
@@ -324,10 +354,13 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc[i][j] = fmaf(av[i], bv[j], acc[i][j]);
     }
-    // epilogue: ds = (|x|^2 + |q|^2) - 2 q.x, keep rows that can reach the bound
     const float4 xn4 = reinterpret_cast<const float4 *>(xs + DIM * BLK)[ty];
+    __syncwarp();
+    if (lane == 0) mbar_arrive(&sm.empty[st]);  // this warp is done with the slot
+    // epilogue: ds = (|x|^2 + |q|^2) - 2 q.x; keep rows that can reach the bound
     const float xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
     const uint32_t row0 = (it.blk0 + sub) * BLK + ty * 4;
+    uint32_t pass = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       const int L = tx * 8 + j;
@@ -337,34 +370,39 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
 #pragma unroll
       for (int i = 0; i < 4; ++i) {
         const float ds = fmaf(-2.f, acc[i][j], xn[i] + qn);
+        acc[i][j] = ds;
         const uint32_t p = row0 + i;
-        if (ds <= pl && p >= s && p < e) {
-          const int idx = atomicAdd(&sm.cnt[L], 1);
-          Candidate c;
-          c.ds = ds;
-          c.pos = p;
-          out_item[(uint64_t)L * CAP + idx] = c;
-        }
+        pass |= (uint32_t)(ds <= pl && p >= s && p < e) << (j * 4 + i);
       }
     }
-    __syncthreads();
-    if (tid == 0 && sub + SC_STAGES < nsub) {
-      fence_proxy_async();
-      mbar_arrive_expect_tx(&sm.bar[st], BLK_BYTES);
-      bulk_g2s(sm.xs[st], blocks + (uint64_t)(it.blk0 + sub + SC_STAGES) * BLK_FLOATS, BLK_BYTES, &sm.bar[st]);
+    if (__any_sync(0xffffffffu, pass != 0)) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          if (pass & (1u << (j * 4 + i))) {
+            const int L = tx * 8 + j;
+            const int idx = atomicAdd(&sm.cnt[L], 1);
+            Candidate c;
+            c.ds = acc[i][j];
+            c.pos = row0 + i;
+            out_item[(uint64_t)L * CAP + idx] = c;
+          }
+        }
+      }
+      __syncwarp();
     }
-    // lists near capacity are compacted; bounds refreshed from other CTAs
-    const bool refresh = (sub % SC_REFRESH) == SC_REFRESH - 1;
+    // own lists near capacity are compacted; bounds refreshed from other CTAs
     {
-      const int L = warp + 4 * (lane & 15);
+      const int L = 16 * warp + (lane & 15);
       const bool need = lane < 16 && sm.cnt[L] > CAP - BLK;
       uint32_t m = __ballot_sync(0xffffffffu, need);
       while (m) {
         const int b = __ffs(m) - 1;
         m &= m - 1;
-        compact_list(out_item + (uint64_t)(warp + 4 * b) * CAP, sm, warp + 4 * b, k, T_global, ovf);
+        compact_list(out_item + (uint64_t)(16 * warp + b) * CAP, sm, 16 * warp + b, k, T_global, ovf);
       }
-      if (refresh && lane < 16 && !need) {
+      if ((sub % SC_REFRESH) == SC_REFRESH - 1 && lane < 16 && !need) {
         const int32_t qi = sm.lq[L];
         if (qi >= 0 && sm.push[L] != -INFINITY) {
           const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
@@ -374,31 +412,25 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
           }
         }
       }
+      __syncwarp();
     }
-    __syncthreads();
   }
   if (!ok) {
-    // A bulk copy never landed (bounded wait gave up): give the copies still
-    // in flight a second bounded wait, then mark every query of the tile so
-    // the exact scan answers them.
-    if (tid == 0) {
-      for (uint32_t s = 0; s < SC_STAGES && s < nsub; ++s) {
-        for (uint32_t itr = 0; itr < WAIT_LIMIT; ++itr)
-          if (mbar_try_wait(&sm.bar[s], 0) && mbar_try_wait(&sm.bar[s], 1)) break;
-      }
+    // A bulk copy never landed (bounded wait gave up): this warp's queries
+    // are answered by the exact scan instead.
+    if (lane < 16) {
+      const int L = 16 * warp + lane;
+      if (sm.lq[L] >= 0) ovf[sm.lq[L]] = 1u;
+      out_cnt[(uint64_t)item_id * TQ + L] = 0;
     }
-    if (tid < TQ && sm.lq[tid] >= 0) ovf[sm.lq[tid]] = 1u;
-    __syncthreads();
-    if (tid < TQ) out_cnt[(uint64_t)item_id * TQ + tid] = 0;
     return;
   }
-  // final trim of every non-empty list
+  // final trim of this warp's non-empty lists
   for (int b = 0; b < 16; ++b) {
-    const int L = warp + 4 * b;
+    const int L = 16 * warp + b;
     if (sm.cnt[L] > 0) compact_list(out_item + (uint64_t)L * CAP, sm, L, k, T_global, ovf);
   }
-  __syncthreads();
-  if (tid < TQ) out_cnt[(uint64_t)item_id * TQ + tid] = (uint32_t)sm.cnt[tid];
+  if (lane < 16) out_cnt[(uint64_t)item_id * TQ + 16 * warp + lane] = (uint32_t)sm.cnt[16 * warp + lane];
 }
 
 // --------------------------------------------------------------- merge --
@@ -725,28 +757,18 @@ int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *cou
   return FKNN_OK;
 }
 
-namespace {
-
-struct Plan {
-  std::vector<uint32_t> small;                 // query ids for the exact scan
-  std::vector<uint32_t> big, big_tile, big_lane;
-  std::vector<Tile> tiles;
-  std::vector<WorkItem> items;
-  std::vector<int32_t> lane_q;
-  std::vector<uint32_t> lane_s, lane_e;
-  uint64_t pairs_screened = 0, pairs_passing = 0, pairs_contraction = 0;
-};
-
 // Groups queries into 64-query tiles whose slabs overlap (same order and
 // predicate class, start bucket, then end), and cuts each tile's union
 // range into row chunks.
-void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, Plan &P) {
+void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, const PlanShape &shape,
+               Plan &P) {
+  const int TQ = shape.tq, BLK = shape.blk_rows;
   std::vector<uint32_t> big;
   big.reserve(nq);
   for (uint32_t i = 0; i < nq; ++i) {
     const uint32_t len = desc[i].e - desc[i].s;
     P.pairs_passing += len;
-    if (len <= (uint32_t)SMALL_SLAB) {
+    if (len <= (uint32_t)shape.small_slab) {
       P.small.push_back(i);
     } else {
       big.push_back(i);
@@ -807,11 +829,15 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
     tt.push_back(t);
     i = j;
   }
-  // chunk size from the total work: aim for >= ~8 items per resident CTA
+  // Row chunks per tile.  Every chunk restarts its candidate bound from the
+  // shared one, so fewer, longer chunks mean fewer candidate pushes; a tile
+  // is split only as far as needed to give every resident CTA slot several
+  // work items (shape.target_items in total), and never below
+  // min_chunk_blocks blocks or above max_items_per_tile chunks.
   uint64_t total_blk = 0;
   for (auto &t : tt) total_blk += (t.E + BLK - 1) / BLK - t.S / BLK;
-  uint64_t cb = total_blk / (148ull * 2 * 8);
-  cb = std::max<uint64_t>(16, std::min<uint64_t>(1024, cb));
+  uint64_t cb = std::max<uint64_t>(1, total_blk / std::max<uint32_t>(1, shape.target_items));
+  cb = std::max<uint64_t>(cb, shape.min_chunk_blocks);
   const size_t ntile = tt.size();
   P.tiles.resize(ntile);
   P.lane_q.assign(ntile * TQ, -1);
@@ -835,7 +861,7 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
     const uint32_t b0 = T.S / BLK, b1 = (T.E + BLK - 1) / BLK;
     P.tiles[t].order = (int32_t)T.order;
     P.tiles[t].nq = T.count;
-    const uint32_t cbt = std::max<uint32_t>((uint32_t)cb, (b1 - b0 + MAX_ITEMS_PER_TILE - 1) / MAX_ITEMS_PER_TILE);
+    const uint32_t cbt = std::max<uint32_t>((uint32_t)cb, (b1 - b0 + shape.max_items_per_tile - 1) / shape.max_items_per_tile);
     for (uint32_t b = b0; b < b1; b += cbt) {
       WorkItem w;
       w.tile = (uint32_t)t;
@@ -846,10 +872,13 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
       P.pairs_screened += (uint64_t)(w.blk1 - w.blk0) * BLK * TQ;
     }
   }
-  // Launch order: items that read the same rows run side by side (L2
-  // reuse).  A tile's items are then spread out; the merge finds them
-  // through the per-tile slot table built in search_exact.
+  // Launch order: longest items first (the grid drains evenly), equal
+  // lengths side by side by row range (L2 reuse of the row blocks).  A
+  // tile's items are then spread out; the merge finds them through the
+  // per-tile slot table built by the caller.
   std::stable_sort(items.begin(), items.end(), [&](const WorkItem &a, const WorkItem &b) {
+    const uint32_t la = a.blk1 - a.blk0, lb = b.blk1 - b.blk0;
+    if (la != lb) return la > lb;
     if (P.tiles[a.tile].order != P.tiles[b.tile].order) return P.tiles[a.tile].order < P.tiles[b.tile].order;
     return a.blk0 < b.blk0;
   });
@@ -863,13 +892,10 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
   P.items = std::move(items);
 }
 
-}  // namespace
-
-int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
-                 float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,
+                    QueryDesc **d_desc_out, QueryDesc **h_desc_out, float **h_meta_out) {
   const uint64_t n = idx->n;
   int rc;
-  // 1. validate + resolve slabs
   QueryDesc *d_desc;
   if ((rc = ws_get(idx, 2, (size_t)nq * sizeof(QueryDesc), (void **)&d_desc))) return rc;
   if ((rc = validate_queries(idx, d_q, d_meta, nq, st))) return rc;
@@ -887,11 +913,49 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
   FKNN_CUDA(cudaMemcpyAsync(h_meta, d_meta, (size_t)nq * 16, cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
   if ((rc = check_query_flag(*h_flag))) return rc;
+  *d_desc_out = d_desc;
+  *h_desc_out = h_desc;
+  *h_meta_out = h_meta;
+  return FKNN_OK;
+}
+
+int launch_exact_scan(fknn_index *idx, const uint32_t *list, const uint32_t *d_count, uint32_t h_count, unsigned grid,
+                      const QueryDesc *desc, const float *q, uint32_t k, uint32_t *ids, float *dists, cudaStream_t st) {
+  const OrderData &OT = idx->ord[ORDER_TIME], &OC = idx->ord[ORDER_CAT];
+  k_exact_scan<<<grid, ES_THREADS, 0, st>>>(list, d_count, h_count, desc, q, OT.blocks, OC.blocks, OT.perm, OC.perm, k,
+                                            ids, dists);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int launch_fill_u32(uint32_t *p, uint32_t n, uint32_t v, cudaStream_t st) {
+  k_fill_u32<<<std::min<uint32_t>((n + 255) / 256, 1024), 256, 0, st>>>(p, n, v);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
+                 float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  const uint64_t n = idx->n;
+  int rc;
+  // 1. validate + resolve slabs
+  QueryDesc *d_desc, *h_desc;
+  float *h_meta;
+  if ((rc = prepare_queries(idx, d_q, d_meta, nq, st, &d_desc, &h_desc, &h_meta))) return rc;
 
   // 2. plan
   auto t0 = std::chrono::steady_clock::now();
   Plan P;
-  make_plan(h_desc, h_meta, nq, n, P);
+  PlanShape shape;
+  shape.tq = TQ;
+  shape.blk_rows = BLK;
+  shape.small_slab = SMALL_SLAB;
+  shape.max_items_per_tile = MAX_ITEMS_PER_TILE;
+  shape.min_chunk_blocks = 16;
+  shape.target_items = 148 * 2 * 8;
+  make_plan(h_desc, h_meta, nq, n, shape, P);
   auto t1 = std::chrono::steady_clock::now();
   const uint32_t ntile = (uint32_t)P.tiles.size(), nitems = (uint32_t)P.items.size();
   const uint32_t nbig = (uint32_t)P.big.size(), nsmall = (uint32_t)P.small.size();

@@ -105,6 +105,30 @@ struct Candidate {
   uint32_t pos;
 };
 
+// Host plan of one search call: which queries take the row-by-row exact
+// scan, and the query tiles / row-chunk work items of the contraction.
+struct Plan {
+  std::vector<uint32_t> small;                 // query ids for the exact scan
+  std::vector<uint32_t> big, big_tile, big_lane;
+  std::vector<Tile> tiles;
+  std::vector<WorkItem> items;
+  std::vector<int32_t> lane_q;
+  std::vector<uint32_t> lane_s, lane_e;
+  uint64_t pairs_screened = 0, pairs_passing = 0, pairs_contraction = 0;
+};
+
+struct PlanShape {
+  int tq;                   // queries per tile
+  int blk_rows;             // rows per layout block of the order
+  uint32_t small_slab;      // slabs up to this size take the exact scan
+  uint32_t max_items_per_tile;
+  uint32_t min_chunk_blocks;
+  uint32_t target_items;    // work items wanted in total (several per resident CTA slot)
+};
+
+void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, const PlanShape &shape,
+               Plan &P);
+
 // Device data of one row order.
 struct OrderData {
   float *blocks = nullptr;     // [nblk][101][64]
@@ -175,6 +199,16 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
 int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d_counts, cudaStream_t st);
 int filter_rows(fknn_index *idx, const float *meta4_host, uint32_t *d_out, uint64_t *count, cudaStream_t st);
 int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st);
+int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,
+                    QueryDesc **d_desc, QueryDesc **h_desc, float **h_meta);
+int launch_exact_scan(fknn_index *idx, const uint32_t *list, const uint32_t *d_count, uint32_t h_count, unsigned grid,
+                      const QueryDesc *desc, const float *q, uint32_t k, uint32_t *ids, float *dists, cudaStream_t st);
+int launch_fill_u32(uint32_t *p, uint32_t n, uint32_t v, cudaStream_t st);
+
+// reduced-precision search (bf16_search.cu)
+int build_bf16(fknn_index *idx, cudaStream_t st);
+int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+                uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 
 // launch counter (kernels launched by this library in the current call)
 extern thread_local uint32_t g_launches;

@@ -187,3 +187,22 @@ def recall_at_k(knn: np.ndarray, gt: np.ndarray) -> float:
     for i in range(nq):
         hits += len(np.intersect1d(knn[i], gt[i], assume_unique=False))
     return hits / (nq * k)
+
+
+def recall_matrix(knn: np.ndarray, gt: np.ndarray, pad: int = 0xFFFFFFFF) -> float:
+    """Mean per-query recall of knn against gt (both (nq, k) uint32), padding
+    ids excluded; queries whose gt holds no valid id are skipped."""
+    knn = np.asarray(knn, dtype=np.uint64)
+    gt = np.asarray(gt, dtype=np.uint64)
+    nq, k = gt.shape
+    rows = np.arange(nq, dtype=np.uint64)[:, None] << np.uint64(32)
+    gv = gt != pad
+    a = (knn + rows)[knn != pad]
+    b = (gt + rows)[gv]
+    hit = np.zeros(gt.shape, dtype=bool)
+    hit[gv] = np.isin(b, a)
+    nvalid = gv.sum(axis=1)
+    m = nvalid > 0
+    if not m.any():
+        return 1.0
+    return float(np.mean(hit.sum(axis=1)[m] / nvalid[m]))
