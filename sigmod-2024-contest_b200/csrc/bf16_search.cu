@@ -19,6 +19,7 @@
 #include <cstring>
 
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 
 #include "device_util.cuh"
 
@@ -28,16 +29,45 @@ namespace {
 
 constexpr int BQ = 128;                       // queries per tile = MMA M = TMEM lanes
 constexpr int BR = 128;                       // rows per sub-tile = MMA N
-constexpr int BK = 112;                       // padded K
-constexpr uint32_t BF_TILE = BQ * BK * 2;     // 28672 bytes, both operands
 constexpr int BS = 2;                         // shared-memory stages for row blocks
 constexpr int B_EPI_WARPS = 4;
 constexpr int B_THREADS = (2 + B_EPI_WARPS) * 32;  // producer, MMA issuer, 4 epilogue warps
 constexpr uint32_t TMEM_COLS = 2 * BR;        // double-buffered accumulator
 
-__host__ __device__ __forceinline__ uint32_t cm_index(uint32_t r, uint32_t k) {
-  return ((k >> 3) * (BQ / 8) + (r >> 3)) * 64 + (r & 7) * 8 + (k & 7);
+// Operand formats of the tensor-core screen.  Both operands are K-major,
+// no swizzle, in core matrices of 8 rows x 16 bytes; every MMA consumes 32
+// bytes of K per row (two core-matrix columns), so the descriptors of both
+// formats are alike and only the MMA kind, its K and the bytes per row differ.
+struct FmtBF16 {
+  static constexpr bool kFP8 = false;
+  static constexpr int K = 112;                 // 100 dims, 2 norm terms, zero padding
+  static constexpr int ROW_BYTES = K * 2;
+  static constexpr int MMAS = K / 16;           // kind::f16: K = 16 per MMA
+  // F32 accumulate, BF16 A and B, K-major, N = BR, M = BQ
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BR >> 3) << 17) | ((uint32_t)(BQ >> 4) << 24);
+};
+struct FmtFP8 {
+  static constexpr bool kFP8 = true;
+  static constexpr int K = 128;                 // 100 dims, 3 norm terms, zero padding
+  static constexpr int ROW_BYTES = K;
+  static constexpr int MMAS = K / 32;           // kind::f8f6f4: K = 32 per MMA
+  // F32 accumulate, E4M3 A and B, K-major, N = BR, M = BQ
+  static constexpr uint32_t IDESC =
+      (1u << 4) | (0u << 7) | (0u << 10) | ((uint32_t)(BR >> 3) << 17) | ((uint32_t)(BQ >> 4) << 24);
+};
+template <class F>
+struct Tiles {
+  static constexpr uint32_t BYTES = (uint32_t)BQ * F::ROW_BYTES;  // one 128-row operand tile
+};
+constexpr uint32_t BF_TILE = Tiles<FmtBF16>::BYTES;  // 28672
+constexpr uint32_t F8_TILE = Tiles<FmtFP8>::BYTES;   // 16384
+
+// byte offset of (row r, byte b of the row) in a 128-row core-matrix tile
+__host__ __device__ __forceinline__ uint32_t cm_byte(uint32_t r, uint32_t b) {
+  return ((b >> 4) * (BQ / 8) + (r >> 3)) * 128 + (r & 7) * 16 + (b & 15);
 }
+__host__ __device__ __forceinline__ uint32_t cm_index(uint32_t r, uint32_t k) { return cm_byte(r, 2 * k) / 2; }
 
 // ------------------------------------------------------------ tcgen05 --
 
@@ -50,15 +80,19 @@ __device__ __forceinline__ uint64_t umma_desc(uint32_t saddr, uint32_t lbo, uint
   return d;
 }
 
-// kind::f16 instruction descriptor: F32 accumulate, BF16 A and B, both K-major.
-constexpr uint32_t IDESC_BF16 =
-    (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(BR >> 3) << 17) | ((uint32_t)(BQ >> 4) << 24);
-
-__device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
-  asm volatile(
-      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
-      " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
-      "l"(da), "l"(db), "r"(IDESC_BF16), "r"(accumulate));
+template <class F>
+__device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  if constexpr (F::kFP8) {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(F::IDESC), "r"(accumulate));
+  } else {
+    asm volatile(
+        "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+        " tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+        "l"(da), "l"(db), "r"(F::IDESC), "r"(accumulate));
+  }
 }
 
 __device__ __forceinline__ void umma_commit(uint64_t *bar) {
@@ -93,6 +127,7 @@ __device__ __forceinline__ void mbar_arrive1(uint64_t *bar) {
 __global__ void k_build_bf16_blocks(const float *__restrict__ vecs, const float *__restrict__ norms,
                                     const uint32_t *__restrict__ perm, uint64_t n, __nv_bfloat16 *__restrict__ out) {
   const uint64_t b = blockIdx.x;
+  constexpr int BK = FmtBF16::K;
   __nv_bfloat16 *o = out + b * (BF_TILE / 2);
   for (uint32_t i = threadIdx.x; i < (uint32_t)BR * BK; i += blockDim.x) {
     const uint32_t r = i / BK, k = i % BK;
@@ -113,9 +148,15 @@ __global__ void k_build_bf16_blocks(const float *__restrict__ vecs, const float 
 }
 
 __global__ void k_tile_stage_bf16(const float *__restrict__ q, const int32_t *__restrict__ lane_q,
-                                  __nv_bfloat16 *__restrict__ out) {
+                                  const QueryDesc *__restrict__ desc, __nv_bfloat16 *__restrict__ out,
+                                  float2 *__restrict__ lane_qs) {
+  constexpr int BK = FmtBF16::K;
   const uint32_t t = blockIdx.x;
   __nv_bfloat16 *o = out + (uint64_t)t * (BF_TILE / 2);
+  for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
+    const int32_t qi = lane_q[t * BQ + l];
+    lane_qs[t * BQ + l] = make_float2(qi >= 0 ? desc[qi].qn : 0.f, 1.f);
+  }
   for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * BK; i += blockDim.x) {
     const uint32_t l = i / BK, k = i % BK;
     const int32_t qi = lane_q[t * BQ + l];
@@ -128,11 +169,128 @@ __global__ void k_tile_stage_bf16(const float *__restrict__ q, const int32_t *__
   }
 }
 
+// FP8-e4m3 per-dimension-scaled codes, the tensor-core analogue of the
+// per-dimension SQ8 codes of sq8_quant.hpp:30-63 (mi/dif per dimension).
+// Each dimension is centred at c = (max + min)/2 and scaled by
+// s = (max - min)/2 / 448 so its range fills e4m3 (|x'| <= 448):
+//   row side : x'_k = e4m3((x_k - c_k) / s_k), k < 100; dims 100..102 hold
+//              -|x - c|^2/2 as e4m3 high, middle and low parts
+//   query    : A_k = e4m3(lambda * (q_k - c_k) * s_k); dims 100..102 = lambda,
+//              lambda a power of two in [2^-9, 2^8] with max|A_k| <= 448
+// so acc = lambda * ((q - c).(x - c) - |x - c|^2/2) and
+// ds = |q - c|^2 - 2 acc / lambda approximates |q - x|^2.
+__global__ void k_dim_minmax(const float *__restrict__ vecs, uint64_t n, uint32_t *__restrict__ mn,
+                             uint32_t *__restrict__ mx) {
+  __shared__ uint32_t smn[DIM], smx[DIM];
+  for (int d = threadIdx.x; d < DIM; d += blockDim.x) {
+    smn[d] = 0xffffffffu;
+    smx[d] = 0u;
+  }
+  __syncthreads();
+  const uint64_t total = n * DIM;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < total; i += (uint64_t)gridDim.x * blockDim.x) {
+    const uint32_t u = f32_sortable(vecs[i]);
+    const int d = (int)(i % DIM);
+    atomicMin(&smn[d], u);
+    atomicMax(&smx[d], u);
+  }
+  __syncthreads();
+  for (int d = threadIdx.x; d < DIM; d += blockDim.x) {
+    atomicMin(&mn[d], smn[d]);
+    atomicMax(&mx[d], smx[d]);
+  }
+}
+
+__global__ void k_fp8_params(const uint32_t *__restrict__ mn, const uint32_t *__restrict__ mx,
+                             float *__restrict__ center, float *__restrict__ scale) {
+  const int d = threadIdx.x;
+  if (d >= DIM) return;
+  const float a = sortable_f32(mn[d]), b = sortable_f32(mx[d]);
+  center[d] = 0.5f * (a + b);
+  scale[d] = fmaxf(0.5f * (b - a), 1e-30f) / 448.f;
+}
+
+__global__ void k_build_fp8_blocks(const float *__restrict__ vecs, const uint32_t *__restrict__ perm, uint64_t n,
+                                   const float *__restrict__ center, const float *__restrict__ scale,
+                                   unsigned char *__restrict__ out) {
+  const uint64_t b = blockIdx.x;
+  unsigned char *o = out + b * F8_TILE;
+  __shared__ float cn[BR];
+  // centred norms of the block's rows (float FMA chain)
+  for (uint32_t r = threadIdx.x; r < (uint32_t)BR; r += blockDim.x) {
+    const uint64_t p = b * BR + r;
+    float s = 0.f;
+    if (p < n) {
+      const float *x = vecs + (uint64_t)perm[p] * DIM;
+      for (int k = 0; k < DIM; ++k) {
+        const float t = x[k] - center[k];
+        s = fmaf(t, t, s);
+      }
+    }
+    cn[r] = s;
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < (uint32_t)BR * FmtFP8::K; i += blockDim.x) {
+    const uint32_t r = i / FmtFP8::K, k = i % FmtFP8::K;
+    const uint64_t p = b * BR + r;
+    float v = 0.f;
+    if (p < n) {
+      if (k < (uint32_t)DIM) {
+        v = (vecs[(uint64_t)perm[p] * DIM + k] - center[k]) / scale[k];
+      } else if (k <= DIM + 2) {
+        const float h = -0.5f * cn[r];
+        const float hi = float(__nv_fp8_e4m3(h));
+        const float mid = float(__nv_fp8_e4m3(h - hi));
+        v = (k == DIM) ? hi : (k == DIM + 1) ? mid : h - hi - mid;
+      }
+    }
+    o[cm_byte(r, k)] = __nv_fp8_e4m3(v).__x;
+  }
+}
+
+__global__ void k_tile_stage_fp8(const float *__restrict__ q, const int32_t *__restrict__ lane_q,
+                                 const float *__restrict__ center, const float *__restrict__ scale,
+                                 unsigned char *__restrict__ out, float2 *__restrict__ lane_qs) {
+  const uint32_t t = blockIdx.x;
+  unsigned char *o = out + (uint64_t)t * F8_TILE;
+  __shared__ float lam[BQ];
+  for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
+    const int32_t qi = lane_q[t * BQ + l];
+    float qn = 0.f, mw = 0.f;
+    if (qi >= 0) {
+      const float *x = q + (uint64_t)qi * DIM;
+      for (int k = 0; k < DIM; ++k) {
+        const float u = x[k] - center[k];
+        qn = fmaf(u, u, qn);
+        mw = fmaxf(mw, fabsf(u * scale[k]));
+      }
+    }
+    // largest power of two with lambda * max|w| <= 448, within e4m3's exact powers
+    int e = 8;
+    if (mw > 0.f) e = min(8, max(-9, (int)floorf(log2f(448.f / mw))));
+    const float lambda = ldexpf(1.f, e);
+    lam[l] = lambda;
+    lane_qs[t * BQ + l] = make_float2(qn, 1.f / lambda);
+  }
+  __syncthreads();
+  for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * FmtFP8::K; i += blockDim.x) {
+    const uint32_t l = i / FmtFP8::K, k = i % FmtFP8::K;
+    const int32_t qi = lane_q[t * BQ + l];
+    float v = 0.f;
+    if (qi >= 0) {
+      if (k < (uint32_t)DIM) v = lam[l] * (q[(uint64_t)qi * DIM + k] - center[k]) * scale[k];
+      else if (k <= DIM + 2) v = lam[l];
+    }
+    o[cm_byte(l, k)] = __nv_fp8_e4m3(v).__x;
+  }
+}
+
 // ------------------------------------------------------------ screen ---
 
+template <class F>
 struct BScreenSmem {
-  unsigned char a[BF_TILE];
-  unsigned char b[BS][BF_TILE];
+  unsigned char a[Tiles<F>::BYTES];
+  unsigned char b[BS][Tiles<F>::BYTES];
   float thr[BQ];  // current k'-th screening distance bound T
   float qn[BQ];
   int cnt[BQ];
@@ -195,7 +353,8 @@ __device__ float warp_select_kth(const Candidate *list, int n, int kth, uint32_t
 }
 
 // Bound and trim list L to its k' smallest screening distances (ties kept).
-__device__ __noinline__ void bcompact(Candidate *list, BScreenSmem &sm, int L, int wslot, uint32_t kprime,
+template <class F>
+__device__ __noinline__ void bcompact(Candidate *list, BScreenSmem<F> &sm, int L, int wslot, uint32_t kprime,
                                       uint32_t capb, uint32_t *T_global, uint32_t *ovf) {
   const int lane = threadIdx.x & 31;
   const int n = sm.cnt[L];
@@ -235,16 +394,18 @@ __device__ __noinline__ void bcompact(Candidate *list, BScreenSmem &sm, int L, i
   __syncwarp();
 }
 
+template <class F>
 __global__ void __launch_bounds__(B_THREADS, 2)
-    k_screen_bf16(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles,
+    k_screen_tc(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles,
                   const unsigned char *__restrict__ atiles, const int32_t *__restrict__ lane_q,
                   const uint32_t *__restrict__ lane_s, const uint32_t *__restrict__ lane_e,
-                  const QueryDesc *__restrict__ desc, const unsigned char *__restrict__ blocks_t,
+                  const float2 *__restrict__ lane_qs, const unsigned char *__restrict__ blocks_t,
                   const unsigned char *__restrict__ blocks_c, uint32_t *__restrict__ T_global,
                   uint32_t *__restrict__ ovf, Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt,
                   uint32_t kprime, uint32_t capb, int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
-  BScreenSmem &sm = *reinterpret_cast<BScreenSmem *>(smem_raw);
+  BScreenSmem<F> &sm = *reinterpret_cast<BScreenSmem<F> *>(smem_raw);
+  constexpr uint32_t TB = Tiles<F>::BYTES;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const uint32_t item_id = blockIdx.x;
   const WorkItem it = items[item_id];
@@ -277,14 +438,14 @@ __global__ void __launch_bounds__(B_THREADS, 2)
   if (warp == 0) {
     // ------------------------------------------------ producer
     if (lane == 0) {
-      mbar_arrive_expect_tx(&sm.abar, BF_TILE);
-      bulk_g2s(sm.a, atiles + (uint64_t)it.tile * BF_TILE, BF_TILE, &sm.abar);
+      mbar_arrive_expect_tx(&sm.abar, TB);
+      bulk_g2s(sm.a, atiles + (uint64_t)it.tile * TB, TB, &sm.abar);
       uint32_t issued = 0;
       for (uint32_t sub = 0; sub < nsub; ++sub) {
         const int st = sub % BS;
         if (sub >= BS && !mbar_wait_bounded(&sm.empty[st], ((sub / BS) - 1) & 1, err)) break;
-        mbar_arrive_expect_tx(&sm.full[st], BF_TILE);
-        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub) * BF_TILE, BF_TILE, &sm.full[st]);
+        mbar_arrive_expect_tx(&sm.full[st], TB);
+        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub) * TB, TB, &sm.full[st]);
         ++issued;
       }
       mbar_wait_bounded(&sm.abar, 0, err);
@@ -304,10 +465,10 @@ __global__ void __launch_bounds__(B_THREADS, 2)
           tc_fence_after();
           const uint32_t b0 = smem_u32(sm.b[st]);
 #pragma unroll
-          for (int kk = 0; kk < BK / 16; ++kk) {
+          for (int kk = 0; kk < F::MMAS; ++kk) {
             const uint64_t da = umma_desc(a0 + kk * 2 * (BQ / 8) * 128, (BQ / 8) * 128, 128);
             const uint64_t db = umma_desc(b0 + kk * 2 * (BR / 8) * 128, (BR / 8) * 128, 128);
-            umma_bf16(tmem + ab * BR, da, db, kk > 0);
+            umma<F>(tmem + ab * BR, da, db, kk > 0);
           }
           umma_commit(&sm.empty[st]);     // the row block may be overwritten once these MMAs finish
           umma_commit(&sm.accfull[ab]);   // the accumulator is ready for the epilogue
@@ -323,11 +484,12 @@ __global__ void __launch_bounds__(B_THREADS, 2)
     const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
     const int L = wg * 32 + lane;
     const int32_t qi = lane_q[it.tile * BQ + L];
-    float qn = 0.f;
+    // per query: |q|^2 (centred for FP8) and the accumulator's scale 1/lambda
+    const float2 qsc = lane_qs[it.tile * BQ + L];
+    const float qn = qsc.x, sc = qsc.y;
     uint32_t s = 0, e = 0;
     float T = -INFINITY;
     if (qi >= 0) {
-      qn = desc[qi].qn;
       s = lane_s[it.tile * BQ + L];
       e = lane_e[it.tile * BQ + L];
       T = sortable_f32(ld_volatile_u32(T_global + qi));
@@ -350,8 +512,8 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       const uint32_t p0 = (it.blk0 + sub) * BR;
       const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
       const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
-      // candidate iff qn - 2*acc <= T  <=>  acc >= (qn - T) / 2
-      const float cq = (T == INFINITY) ? -INFINITY : 0.5f * (qn - T);
+      // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc)
+      const float cq = (T == INFINITY) ? -INFINITY : 0.5f * (qn - T) / sc;
 #pragma unroll 1
       for (int c = 0; c < BR; c += 32) {
         float v[32];
@@ -372,7 +534,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
           for (int j = 0; j < 32; ++j) {
             if (v[j] >= cq && c + j >= r0 && c + j < r1) {
               Candidate cd;
-              cd.ds = fmaf(-2.f, v[j], qn);
+              cd.ds = fmaf(-2.f * sc, v[j], qn);
               cd.pos = p0 + c + j;
               list[cnt++] = cd;
             }
@@ -575,9 +737,32 @@ int build_bf16(fknn_index *idx, cudaStream_t st) {
   return FKNN_OK;
 }
 
-int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
-                uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+int build_fp8(fknn_index *idx, cudaStream_t st) {
+  const uint64_t nblk = (idx->n + BR - 1) / BR;
+  int rc = dev_alloc(idx, (void **)&idx->fp8_scale, 2 * DIM * sizeof(float));  // centre[100], scale[100]
+  if (rc) return rc;
+  uint32_t *mm;
+  if ((rc = ws_get(idx, 15, 2 * DIM * sizeof(uint32_t), (void **)&mm))) return rc;
+  FKNN_CUDA(cudaMemsetAsync(mm, 0xff, DIM * sizeof(uint32_t), st));
+  FKNN_CUDA(cudaMemsetAsync(mm + DIM, 0, DIM * sizeof(uint32_t), st));
+  k_dim_minmax<<<148 * 4, 256, 0, st>>>(idx->vecs, idx->n, mm, mm + DIM);
+  k_fp8_params<<<1, 128, 0, st>>>(mm, mm + DIM, idx->fp8_scale, idx->fp8_scale + DIM);
+  g_launches += 2;
+  for (int o = 0; o < 2; ++o) {
+    if ((rc = dev_alloc(idx, &idx->fp8_blocks[o], nblk * F8_TILE))) return rc;
+    k_build_fp8_blocks<<<(unsigned)nblk, 256, 0, st>>>(idx->vecs, idx->ord[o].perm, idx->n, idx->fp8_scale,
+                                                       idx->fp8_scale + DIM, (unsigned char *)idx->fp8_blocks[o]);
+    g_launches += 1;
+  }
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+template <class F>
+static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+                     uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
   const uint64_t n = idx->n;
+  constexpr uint32_t TB = Tiles<F>::BYTES;
   int rc;
   QueryDesc *d_desc, *h_desc;
   float *h_meta;
@@ -650,24 +835,32 @@ int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t
     unsigned char *d_at;
     Candidate *d_out;
     uint32_t *d_ocnt;
-    if ((rc = ws_get(idx, 4, (size_t)ntile * BF_TILE, (void **)&d_at))) return rc;
+    float2 *d_lqs;
+    if ((rc = ws_get(idx, 4, (size_t)ntile * TB, (void **)&d_at))) return rc;
+    if ((rc = ws_get(idx, 10, (size_t)ntile * BQ * sizeof(float2), (void **)&d_lqs))) return rc;
     if ((rc = ws_get(idx, 6, (size_t)nitems * BQ * capb * sizeof(Candidate), (void **)&d_out))) return rc;
     if ((rc = ws_get(idx, 7, (size_t)nitems * BQ * 4, (void **)&d_ocnt))) return rc;
-    k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), (__nv_bfloat16 *)d_at);
+    if constexpr (F::kFP8)
+      k_tile_stage_fp8<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), idx->fp8_scale,
+                                              idx->fp8_scale + DIM, d_at, d_lqs);
+    else
+      k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), d_desc, (__nv_bfloat16 *)d_at,
+                                               d_lqs);
     static bool attr = false;
     if (!attr) {
-      FKNN_CUDA(cudaFuncSetAttribute(k_screen_bf16, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(BScreenSmem)));
+      FKNN_CUDA(cudaFuncSetAttribute(k_screen_tc<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)sizeof(BScreenSmem<F>)));
       FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                      (int)sizeof(RerankSmem)));
       attr = true;
     }
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
-    k_screen_bf16<<<nitems, B_THREADS, sizeof(BScreenSmem), st>>>(
+    void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
+    k_screen_tc<F><<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
-        (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_desc,
-        (const unsigned char *)idx->bf16_blocks[ORDER_TIME], (const unsigned char *)idx->bf16_blocks[ORDER_CAT],
-        T_global, ovf, d_out, d_ocnt, kprime, capb, idx->d_flag);
+        (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_lqs,
+        (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
+        d_ocnt, kprime, capb, idx->d_flag);
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     k_merge_rerank<<<nbig, RR_THREADS, sizeof(RerankSmem), st>>>(
         (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
@@ -710,6 +903,16 @@ int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t
     stats->n_boundary_f64 = h2[1];
   }
   return FKNN_OK;
+}
+
+int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+                uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  return search_tc<FmtBF16>(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+}
+
+int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+               uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  return search_tc<FmtFP8>(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
 }
 
 }  // namespace fknn

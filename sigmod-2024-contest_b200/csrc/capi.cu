@@ -177,8 +177,11 @@ int fknn_index_create(const float *vecs, const float *labels, const float *ts, u
     }
   }
   if (!rc && opts && opts->build_fp8) {
-    set_error("fknn_index_create: FP8 codes are not available in this build");
-    rc = FKNN_EUNSUPPORTED;
+    rc = build_fp8(idx, idx->own_stream);
+    if (!rc) {
+      cudaError_t e2 = cudaStreamSynchronize(idx->own_stream);
+      if (e2 != cudaSuccess) rc = cuda_fail(e2, "build_fp8");
+    }
   }
   // build temporaries are not needed by searches
   for (int s = 10; s < 16; ++s) {
@@ -228,9 +231,10 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     return FKNN_EINVAL;
   }
   const uint32_t kprime = (opts && opts->kprime) ? opts->kprime : 400;
-  if (mode == FKNN_MODE_BF16_RERANK) {
-    if (!idx->bf16_blocks[0]) {
-      set_error("fknn_search: BF16 mode needs an index created with build_bf16");
+  if (mode == FKNN_MODE_BF16_RERANK || mode == FKNN_MODE_FP8_RERANK) {
+    if (mode == FKNN_MODE_BF16_RERANK ? !idx->bf16_blocks[0] : !idx->fp8_blocks[0]) {
+      set_error(mode == FKNN_MODE_BF16_RERANK ? "fknn_search: BF16 mode needs an index created with build_bf16"
+                                             : "fknn_search: FP8 mode needs an index created with build_fp8");
       return FKNN_EUNSUPPORTED;
     }
     if (kprime < k || kprime > 1024) {
@@ -262,8 +266,12 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     if ((rc = ws_get(idx, 8, (size_t)nq * k * 4, (void **)&d_ids))) return rc;
   if (dists && !dd_dev)
     if ((rc = ws_get(idx, 9, (size_t)nq * k * 4, (void **)&d_dists))) return rc;
-  rc = mode == FKNN_MODE_BF16_RERANK ? search_bf16(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats)
-                                     : search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
+  if (mode == FKNN_MODE_BF16_RERANK)
+    rc = search_bf16(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+  else if (mode == FKNN_MODE_FP8_RERANK)
+    rc = search_fp8(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+  else
+    rc = search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
   if (rc) return rc;
   if (!i_dev) FKNN_CUDA(cudaMemcpyAsync(ids, d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && !dd_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_dists, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));

@@ -207,6 +207,9 @@ int launch_fill_u32(uint32_t *p, uint32_t n, uint32_t v, cudaStream_t st);
 
 // reduced-precision search (bf16_search.cu)
 int build_bf16(fknn_index *idx, cudaStream_t st);
+int build_fp8(fknn_index *idx, cudaStream_t st);
+int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
+               uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
                 uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 
