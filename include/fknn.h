@@ -18,6 +18,12 @@
  *   fknn_sq8_bruteforce    <- bruteforce(dim, k, ...)                  bruteforce.h:244
  *   fknn_sq8_bruteforce_subgraph <- bruteforce_subgraph(...)           bruteforce.h:267
  *   fknn_sq8_sym_train     <- SQ8SymmetricQuantizer::train/encode      pyglass/glass/quant/sq8_sym_quant.hpp:32-74
+ *   fknn_graph_create      <- Graph::load + create_searcher + SetData  pyglass/glass/graph.hpp:117-137,
+ *                                                                      searcher.hpp:94-101,572-583
+ *   fknn_graph_search      <- Searcher::Search / SearchFilter /
+ *                             SearchFilterSubTime / SearchCategoryRange /
+ *                             SearchRangeFilterSubTime / SearchRangeFilter
+ *                                                                      pyglass/glass/searcher.hpp:162-569
  */
 #ifndef FKNN_H_
 #define FKNN_H_
@@ -165,6 +171,45 @@ int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoint
  * distances[k] = heap distance * alpha * alpha. */
 int fknn_sq8_bruteforce_subgraph(size_t dim, size_t k, int *closest_points, float *distances, size_t npoints,
                                  const char *codes_in, float alpha, size_t nqueries, const int8_t *queries_in);
+
+/* ---- Graph beam search (pyglass Searcher over an HNSW level-0 graph) ---- */
+
+/* Search forms, numbered as the reference's Searcher methods. */
+#define FKNN_GRAPH_SEARCH 0            /* Search(q, k, dst)                         searcher.hpp:162 */
+#define FKNN_GRAPH_FILTER 1            /* SearchFilter(q, k, refine, dst, f)         searcher.hpp:262 */
+#define FKNN_GRAPH_FILTER_SUBTIME 2    /* SearchFilterSubTime (+ dists)              searcher.hpp:377 */
+#define FKNN_GRAPH_CATEGORY_RANGE 3    /* SearchCategoryRange (bounds, id_bounds)    searcher.hpp:301 */
+#define FKNN_GRAPH_RANGE_SUBTIME 4     /* SearchRangeFilterSubTime (+ dists)         searcher.hpp:415 */
+#define FKNN_GRAPH_RANGE 5             /* SearchRangeFilter                          searcher.hpp:493 */
+
+typedef struct fknn_graph fknn_graph;
+
+/* Loads a graph from the bytes Graph::save writes (graph.hpp:101-115: nep,
+ * eps, N, K, N x K neighbour ids with -1 padding, N x K edge timestamps, and
+ * optionally the HNSW upper layers, HNSWInitializer.hpp:73-82) and trains
+ * the searcher's symmetric SQ8 codes on vecs (N x 100 host or device
+ * floats, the graph's own points), as Searcher::SetData does.  The graph
+ * lives on `device`. */
+int fknn_graph_create(const void *graph_bytes, size_t nbytes, const float *vecs, int device, fknn_graph **out);
+int fknn_graph_destroy(fknn_graph *g);
+/* n = points, degree = K of the level-0 graph, alpha = the SQ8 scale. */
+int fknn_graph_info(const fknn_graph *g, uint32_t *n, uint32_t *degree, float *alpha);
+
+/* nq searches of the Searcher form `mode`, one per query, with the
+ * reference's pool (capacity max(k, ef); ef = 0 means the reference's 32),
+ * visiting order and tie rules, so ids equal the reference's on the same
+ * graph.  queries nq x 100; out_ids nq x refine (pool slots 0..refine-1,
+ * as reorder writes them); out_dists nq x refine (slot distance x alpha^2,
+ * as reorder_dist writes them; may be NULL).  bounds (nq x 2 floats, the
+ * timestamp window [l, r]) and id_bounds (nq x 2 ints, the range whose ten
+ * evenly spaced ids seed the pool) are read by modes 3-5 and may be NULL
+ * otherwise.  Mode 0 writes k ids (refine must equal k).  Requires
+ * 1 <= k <= 4096 and 1 <= refine <= max(k, ef) + 1.  Pointers may be host or
+ * device memory; the call waits for `stream`.  A graph handle serves one
+ * call at a time. */
+int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode, uint32_t k, uint32_t ef,
+                      uint32_t refine, const float *bounds, const int32_t *id_bounds, int32_t *out_ids,
+                      float *out_dists, void *stream);
 
 #ifdef __cplusplus
 }

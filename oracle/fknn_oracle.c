@@ -351,3 +351,224 @@ int oracle_sq8_bruteforce(uint64_t k, int32_t *closest, float *dists, uint64_t n
   free(h);
   return 0;
 }
+
+/* ---- Graph beam search: the pyglass Searcher (pyglass/glass/searcher.hpp) ----
+ *
+ * A sequential restatement over a graph in Graph::save's byte layout
+ * (graph.hpp:101-115; initializer HNSWInitializer.hpp:73-82), with the
+ * searcher's SQ8-sym codes (Searcher::SetData, searcher.hpp:94-101).
+ * The visited sets are plain byte arrays, which answer exactly what the
+ * lazily-cleared Bitset (neighbor.hpp:41-102) answers. */
+
+typedef struct {
+  int32_t nep, N, K, upK, ep;
+  const int32_t *eps, *adj;
+  const float *ets;
+  int32_t *levels;
+  const int32_t **lists; /* per node: levels * upK ids */
+} og_graph;
+
+static int og_parse(const uint8_t *b, size_t nbytes, og_graph *g) {
+  size_t off = 0;
+  memset(g, 0, sizeof(*g));
+  g->ep = -1;
+#define OG_NEED(x) do { if ((size_t)(x) > nbytes - off) return -1; } while (0)
+  OG_NEED(4); memcpy(&g->nep, b + off, 4); off += 4;
+  if (g->nep < 0) return -1;
+  OG_NEED((size_t)g->nep * 4); g->eps = (const int32_t *)(b + off); off += (size_t)g->nep * 4;
+  OG_NEED(8); memcpy(&g->N, b + off, 4); memcpy(&g->K, b + off + 4, 4); off += 8;
+  if (g->N <= 0 || g->K <= 0) return -1;
+  size_t nk = (size_t)g->N * g->K;
+  OG_NEED(nk * 8);
+  g->adj = (const int32_t *)(b + off); off += nk * 4;
+  g->ets = (const float *)(b + off); off += nk * 4;
+  if (off == nbytes) return g->nep > 0 ? 0 : -1;
+  int32_t iN;
+  OG_NEED(12); memcpy(&iN, b + off, 4); memcpy(&g->upK, b + off + 4, 4); memcpy(&g->ep, b + off + 8, 4); off += 12;
+  if (iN != g->N || g->upK <= 0) return -1;
+  g->levels = (int32_t *)calloc(g->N, 4);
+  g->lists = (const int32_t **)calloc(g->N, sizeof(int32_t *));
+  if (!g->levels || !g->lists) return -2;
+  for (int32_t i = 0; i < g->N; ++i) {
+    int32_t cur;
+    OG_NEED(4); memcpy(&cur, b + off, 4); off += 4;
+    if (cur < 0 || cur % g->upK) return -1;
+    g->levels[i] = cur / g->upK;
+    OG_NEED((size_t)cur * 4); g->lists[i] = (const int32_t *)(b + off); off += (size_t)cur * 4;
+  }
+#undef OG_NEED
+  return off == nbytes ? 0 : -1;
+}
+
+/* LinearPool (neighbor.hpp:223-283). */
+typedef struct {
+  int size, cur, cap;
+  pq_node *data; /* cap + 1 slots, zeroed */
+  uint8_t *vis, *vis1;
+} og_pool;
+
+static int og_insert(og_pool *p, int32_t u, int32_t d) {
+  if (p->size == p->cap && d >= p->data[p->size - 1].d) return 0;
+  int lo = 0, hi = p->size;
+  while (lo < hi) {
+    int mid = (lo + hi) / 2;
+    if (p->data[mid].d > d) hi = mid; else lo = mid + 1;
+  }
+  memmove(&p->data[lo + 1], &p->data[lo], (size_t)(p->size - lo) * sizeof(pq_node));
+  p->data[lo].d = d;
+  p->data[lo].id = u;
+  if (p->size < p->cap) p->size++;
+  if (lo < p->cur) p->cur = lo;
+  return 1;
+}
+
+static int32_t og_pop(og_pool *p) {
+  p->data[p->cur].id |= (int32_t)0x80000000;
+  int pre = p->cur;
+  while (p->cur < p->size && (p->data[p->cur].id >> 31 & 1)) p->cur++;
+  return p->data[pre].id & 0x7fffffff;
+}
+
+static inline int32_t og_dist(const int8_t *codes, const int8_t *q, int32_t u) {
+  return oracle_l2sqr_sq8_sym(q, codes + (size_t)u * SQ8_CODE);
+}
+
+/* Graph::initialize_search (graph.hpp:90-99) + HNSWInitializer::initialize
+ * (HNSWInitializer.hpp:36-58). */
+static void og_initialize(const og_graph *g, og_pool *p, const int8_t *codes, const int8_t *q) {
+  if (g->ep >= 0) {
+    int32_t u = g->ep;
+    int32_t cur_dist = og_dist(codes, q, u);
+    for (int level = g->levels[u]; level > 0; --level) {
+      int changed = 1;
+      while (changed) {
+        changed = 0;
+        const int32_t *list = g->lists[u] + (size_t)(level - 1) * g->upK;
+        for (int i = 0; i < g->upK && list[i] != -1; ++i) {
+          int32_t v = list[i];
+          int32_t d = og_dist(codes, q, v);
+          if (d < cur_dist) { cur_dist = d; u = v; changed = 1; }
+        }
+      }
+    }
+    og_insert(p, u, cur_dist);
+    p->vis[u] = 1;
+  } else {
+    for (int e = 0; e < g->nep; ++e) og_insert(p, g->eps[e], og_dist(codes, q, g->eps[e]));
+  }
+}
+
+/* SearchImpl / SearchFilterImpl / SearchFilterSubTimeImpl expansion
+ * (searcher.hpp:172-198, 271-299, 386-413). */
+static void og_expand_plain(const og_graph *g, og_pool *p, const int8_t *codes, const int8_t *q, int32_t u) {
+  for (int i = 0; i < g->K; ++i) {
+    int32_t v = g->adj[(size_t)u * g->K + i];
+    if (v == -1) break;
+    if (p->vis[v]) continue;
+    p->vis[v] = 1;
+    og_insert(p, v, og_dist(codes, q, v));
+  }
+}
+
+/* SearchCategoryRangeImpl (rf 1, searcher.hpp:320-374) and
+ * SearchRangeFilter[SubTime]Impl (rf 2, searcher.hpp:438-491, 516-569). */
+static void og_expand_filtered(const og_graph *g, og_pool *p, const int8_t *codes, const int8_t *q, int32_t u,
+                               float l, float r, int rf) {
+  int count1 = 0, count2 = 0;
+  for (int i = 0; i < g->K; ++i) {
+    int32_t v = g->adj[(size_t)u * g->K + i];
+    if (v == -1) break;
+    if (p->vis[v]) continue;
+    count2++;
+    p->vis[v] = 1;
+    float t = g->ets[(size_t)u * g->K + i];
+    if (t < l || t > r) continue;
+    og_insert(p, v, og_dist(codes, q, v));
+    count1++;
+  }
+  for (int i = 0; i < g->K; ++i) {
+    if (count1 >= rf * count2) break;
+    int32_t nei = g->adj[(size_t)u * g->K + i];
+    if (nei == -1) break;
+    if (p->vis1[nei]) continue;
+    p->vis1[nei] = 1;
+    for (int j = 0; j < g->K; ++j) {
+      int32_t v = g->adj[(size_t)nei * g->K + j];
+      if (v == -1) break;
+      if (p->vis[v]) continue;
+      p->vis[v] = 1;
+      float t = g->ets[(size_t)nei * g->K + j];
+      if (t < l || t > r) continue;
+      og_insert(p, v, og_dist(codes, q, v));
+      count1++;
+      if (count1 >= rf * count2) break;
+    }
+  }
+}
+
+/* One batch of Searcher calls.  mode: 0 Search, 1 SearchFilter,
+ * 2 SearchFilterSubTime, 3 SearchCategoryRange, 4 SearchRangeFilterSubTime,
+ * 5 SearchRangeFilter.  k is the reference's pool argument (capacity
+ * max(k, ef)), refine the ids written per query (slots 0..refine-1, as
+ * reorder / reorder_dist write them, sq8_sym_quant.hpp:76-89); dists
+ * (nullable) = slot distance * alpha_square.  codes: n x 112 searcher codes;
+ * qcodes: nq x 112 query codes (Computer's encode).  Returns 0, or -1 for a
+ * malformed graph / arguments, -3 for a seed outside [0, n). */
+int oracle_graph_search(const uint8_t *gbytes, size_t nbytes, const int8_t *codes, float alpha,
+                        const int8_t *qcodes, uint32_t nq, int mode, uint32_t k, uint32_t ef, uint32_t refine,
+                        const float *bounds, const int32_t *id_bounds, int32_t *out_ids, float *out_dists) {
+  og_graph g;
+  int rc = og_parse(gbytes, nbytes, &g);
+  if (rc) { free(g.levels); free((void *)g.lists); return -1; }
+  int cap = (int)(k > ef ? k : ef);
+  if (mode < 0 || mode > 5 || k == 0 || refine == 0 || refine > (uint32_t)cap + 1) {
+    free(g.levels); free((void *)g.lists); return -1;
+  }
+  const float alpha_square = alpha * alpha;
+  og_pool p;
+  p.cap = cap;
+  p.data = (pq_node *)malloc(sizeof(pq_node) * (cap + 1));
+  p.vis = (uint8_t *)malloc(g.N);
+  p.vis1 = (uint8_t *)malloc(g.N);
+  rc = 0;
+  for (uint32_t qi = 0; qi < nq && rc == 0; ++qi) {
+    const int8_t *q = qcodes + (size_t)qi * SQ8_CODE;
+    memset(p.data, 0, sizeof(pq_node) * (cap + 1));
+    memset(p.vis, 0, g.N);
+    memset(p.vis1, 0, g.N);
+    p.size = p.cur = 0;
+    float l = 0.f, r = 0.f;
+    int lb = 0, ub = 0;
+    if (mode >= 3) {
+      l = bounds[2 * qi]; r = bounds[2 * qi + 1];
+      lb = id_bounds[2 * qi]; ub = id_bounds[2 * qi + 1];
+    }
+    float sel = (float)(ub - lb) / (float)g.N;
+    int seeded = mode == 3 || (mode >= 4 && sel < 1);
+    if (seeded) {
+      int interval = (ub - lb) / 10;
+      for (int i = 0; i < 10; ++i) {
+        int point = lb + interval * i;
+        if (point < 0 || point >= g.N) { rc = -3; break; }
+        og_insert(&p, point, og_dist(codes, q, point));
+        p.vis[point] = 1;
+      }
+      if (rc) break;
+    } else if (mode != 4) {
+      og_initialize(&g, &p, codes, q);
+    }
+    while (p.cur < p.size) {
+      int32_t u = og_pop(&p);
+      if (mode == 3) og_expand_filtered(&g, &p, codes, q, u, l, r, 1);
+      else if (mode >= 4) og_expand_filtered(&g, &p, codes, q, u, l, r, 2);
+      else og_expand_plain(&g, &p, codes, q, u);
+    }
+    for (uint32_t i = 0; i < refine; ++i) {
+      out_ids[(size_t)qi * refine + i] = p.data[i].id & 0x7fffffff;
+      if (out_dists) out_dists[(size_t)qi * refine + i] = (float)p.data[i].d * alpha_square;
+    }
+  }
+  free(p.data); free(p.vis); free(p.vis1);
+  free(g.levels); free((void *)g.lists);
+  return rc;
+}

@@ -5,8 +5,9 @@ module, and only as the checker / the timed CPU baseline; the product
 library never calls it.
 
   restatement : oracle/libfknn_oracle.so  (oracle/fknn_oracle.c)
-  reference   : oracle/_ref/libref_exact.so, oracle/_ref/libref_sq8.so, the
-                reference's own code compiled from its sources (oracle/Makefile)
+  reference   : oracle/_ref/libref_exact.so, oracle/_ref/libref_sq8.so,
+                oracle/_ref/libref_graph.so, the reference's own code compiled
+                from its sources (oracle/Makefile)
 """
 from __future__ import annotations
 
@@ -21,11 +22,13 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ORACLE_SO = os.path.join(HERE, "libfknn_oracle.so")
 REF_EXACT_SO = os.path.join(HERE, "_ref", "libref_exact.so")
 REF_SQ8_SO = os.path.join(HERE, "_ref", "libref_sq8.so")
+REF_GRAPH_SO = os.path.join(HERE, "_ref", "libref_graph.so")
 DIM = 100
 
 _o = None
 _re = None
 _rs = None
+_rg = None
 
 
 def build(ref: bool = False) -> None:
@@ -57,6 +60,9 @@ def lib() -> ctypes.CDLL:
         L.oracle_l2sqr_sq8_sym.argtypes = [c_void_p, c_void_p]
         L.oracle_sq8_bruteforce.restype = c_int
         L.oracle_sq8_bruteforce.argtypes = [c_uint64, c_void_p, c_void_p, c_uint64, c_void_p, c_float, c_void_p]
+        L.oracle_graph_search.restype = c_int
+        L.oracle_graph_search.argtypes = [c_void_p, ctypes.c_size_t, c_void_p, c_float, c_void_p, c_uint32, c_int,
+                                          c_uint32, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]
         _o = L
     return _o
 
@@ -143,4 +149,80 @@ def sq8_bruteforce(k, codes, alpha, query, with_dists=False):
                                      codes.ctypes.data, c_float(alpha), query.ctypes.data)
     if rc != 0:
         raise ValueError("oracle_sq8_bruteforce: need 1 <= k <= npoints")
+    return (ids, d) if with_dists else ids
+
+
+def ref_graph() -> ctypes.CDLL | None:
+    """The reference HNSW::Build + Searcher compiled from its sources, or None."""
+    global _rg
+    if _rg is None and os.path.exists(REF_GRAPH_SO):
+        L = ctypes.CDLL(REF_GRAPH_SO)
+        L.ref_hnsw_build.restype = c_int
+        L.ref_hnsw_build.argtypes = [c_void_p, c_void_p, c_int, c_int, c_int, ctypes.c_char_p]
+        L.ref_graph_search.restype = c_int
+        L.ref_graph_search.argtypes = [ctypes.c_char_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
+                                       c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+        _rg = L
+    return _rg
+
+
+def _opt_ptr(a, dt, shape):
+    if a is None:
+        return None, None
+    a = _c(a, dt).reshape(shape)
+    return a, a.ctypes.data
+
+
+def graph_search(graph_bytes, vecs, queries, mode: int, k: int, refine: int, bounds=None, id_bounds=None,
+                 ef: int = 32, with_dists: bool = False):
+    """Restated Searcher (searcher.hpp:162-569) over Graph::save bytes; the
+    searcher's codes are trained on vecs (Searcher::SetData).  Returns ids
+    (nq, refine) int32 [and dists]."""
+    gb = np.frombuffer(bytes(graph_bytes), dtype=np.uint8)
+    alpha, codes = sq8_sym_train(_c(vecs, np.float32).reshape(-1, DIM))
+    qc = sq8_sym_encode(queries, alpha)
+    nq = qc.shape[0]
+    b, bp = _opt_ptr(bounds, np.float32, (nq, 2))
+    ib, ibp = _opt_ptr(id_bounds, np.int32, (nq, 2))
+    ids = np.empty((nq, refine), dtype=np.int32)
+    d = np.empty((nq, refine), dtype=np.float32) if with_dists else None
+    rc = lib().oracle_graph_search(gb.ctypes.data, gb.size, codes.ctypes.data, c_float(alpha), qc.ctypes.data, nq,
+                                   mode, k, ef, refine, bp, ibp, ids.ctypes.data,
+                                   d.ctypes.data if with_dists else None)
+    if rc != 0:
+        raise ValueError(f"oracle_graph_search failed ({rc})")
+    return (ids, d) if with_dists else ids
+
+
+def ref_hnsw_graph(vecs, ts, R: int, efc: int, path: str) -> bytes:
+    """Graph::save bytes of the reference HNSW::Build (out-degree R = 2M)."""
+    R_ = ref_graph()
+    if R_ is None:
+        raise RuntimeError("oracle/_ref/libref_graph.so is not built")
+    vecs, ts = _c(vecs, np.float32), _c(ts, np.float32)
+    rc = R_.ref_hnsw_build(vecs.ctypes.data, ts.ctypes.data, vecs.shape[0], R, efc, path.encode())
+    if rc != 0:
+        raise RuntimeError("ref_hnsw_build failed")
+    with open(path, "rb") as f:
+        return f.read()
+
+
+def ref_graph_search(path: str, vecs, labels, ts, queries, mode: int, k: int, refine: int, bounds=None,
+                     id_bounds=None, with_dists: bool = False):
+    """The reference Searcher itself over the graph saved at path."""
+    R_ = ref_graph()
+    if R_ is None:
+        raise RuntimeError("oracle/_ref/libref_graph.so is not built")
+    vecs, labels, ts = _c(vecs, np.float32), _c(labels, np.float32), _c(ts, np.float32)
+    q = _c(queries, np.float32).reshape(-1, DIM)
+    nq = q.shape[0]
+    b, bp = _opt_ptr(bounds, np.float32, (nq, 2))
+    ib, ibp = _opt_ptr(id_bounds, np.int32, (nq, 2))
+    ids = np.empty((nq, refine), dtype=np.int32)
+    d = np.empty((nq, refine), dtype=np.float32) if with_dists else None
+    rc = R_.ref_graph_search(path.encode(), vecs.ctypes.data, labels.ctypes.data, ts.ctypes.data, vecs.shape[0],
+                             q.ctypes.data, nq, mode, k, refine, bp, ibp, ids.ctypes.data,
+                             d.ctypes.data if with_dists else None)
+    if rc != 0:
+        raise RuntimeError("ref_graph_search failed")
     return (ids, d) if with_dists else ids

@@ -97,3 +97,54 @@ void ref_sq8_bruteforce_subgraph(uint64_t k, int *closest, float *dists, uint64_
 }
 #endif
 }
+
+#ifdef REF_GRAPH
+#include "glass/hnsw/hnsw.hpp"
+#include "glass/searcher.hpp"
+
+extern "C" {
+// HNSW::Build (pyglass/glass/hnsw/hnsw.hpp:33-89) with out-degree R = 2M and
+// efConstruction efc over n x 100 vectors and their timestamps; the level-0
+// graph, per-edge timestamps and the upper-layer initializer are written in
+// Graph::save's format (graph.hpp:101-115) to path.  Returns 0.
+int ref_hnsw_build(const float *data, const float *ts, int n, int R, int efc, const char *path) {
+  glass::HNSW h(100, "L2", R, efc);
+  h.Build((float *)data, (float *)ts, n, n, 0);
+  h.final_graph.save(path);
+  return 0;
+}
+
+// The reference Searcher (searcher.hpp) over a saved graph, with its own
+// SQ8-sym quantizer trained on data (Searcher::SetData).  mode:
+//   0 Search            1 SearchFilter        2 SearchFilterSubTime (dists)
+//   3 SearchCategoryRange (bounds, id_bounds) 4 SearchRangeFilterSubTime (dists)
+//   5 SearchRangeFilter
+// K is the pool capacity argument ("k" of the reference calls), refine the
+// number of ids written per query.
+int ref_graph_search(const char *path, const float *data, const float *labels, const float *ts, int n,
+                     const float *queries, int nq, int mode, int K, int refine, const float *bounds,
+                     const int *id_bounds, int *out_ids, float *out_dists) {
+  glass::Graph<int> g;
+  g.load(path);
+  auto s = glass::create_searcher(std::move(g), "L2");
+  s->SetData(data, (float *)labels, (float *)ts, n, 100);
+  for (int i = 0; i < nq; ++i) {
+    const float *q = queries + (size_t)i * 100;
+    int *dst = out_ids + (size_t)i * refine;
+    float *dd = out_dists ? out_dists + (size_t)i * refine : nullptr;
+    std::pair<float, float> qb(bounds ? bounds[2 * i] : 0.f, bounds ? bounds[2 * i + 1] : 0.f);
+    std::pair<int, int> ib(id_bounds ? id_bounds[2 * i] : 0, id_bounds ? id_bounds[2 * i + 1] : 0);
+    switch (mode) {
+      case 0: s->Search(q, K, dst); break;
+      case 1: s->SearchFilter(q, K, refine, dst, nullptr); break;
+      case 2: s->SearchFilterSubTime(q, K, refine, dst, dd, nullptr); break;
+      case 3: s->SearchCategoryRange(q, K, refine, dst, qb, ib); break;
+      case 4: s->SearchRangeFilterSubTime(q, K, refine, dst, dd, qb, ib); break;
+      case 5: s->SearchRangeFilter(q, K, refine, dst, qb, ib); break;
+      default: return -1;
+    }
+  }
+  return 0;
+}
+}
+#endif

@@ -171,4 +171,26 @@ __device__ __forceinline__ void warp_bitonic_sort(float (&key)[N], uint32_t (&va
   }
 }
 
+// L2SqrSQ8_sym (pyglass/glass/simd/distance.hpp:329-366) as an exact int32
+// over 112-byte codes: |q - c|^2 = |q|^2 + |c|^2 - 2 q.c with dp4a; qw is the
+// query code as 28 words, qq its squared norm.
+__device__ __forceinline__ int sq8_dist(const int *__restrict__ qw, int qq, const int8_t *__restrict__ code) {
+  const int4 *c4 = reinterpret_cast<const int4 *>(code);
+  int cc = 0, qc = 0;
+#pragma unroll
+  for (int w = 0; w < 28 / 4; ++w) {
+    const int4 v = c4[w];
+    cc = __dp4a(v.x, v.x, cc);
+    cc = __dp4a(v.y, v.y, cc);
+    cc = __dp4a(v.z, v.z, cc);
+    cc = __dp4a(v.w, v.w, cc);
+    qc = __dp4a(qw[4 * w + 0], v.x, qc);
+    qc = __dp4a(qw[4 * w + 1], v.y, qc);
+    qc = __dp4a(qw[4 * w + 2], v.z, qc);
+    qc = __dp4a(qw[4 * w + 3], v.w, qc);
+  }
+  return qq + cc - 2 * qc;
+}
+
+
 }  // namespace fknn

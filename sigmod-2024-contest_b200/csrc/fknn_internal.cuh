@@ -213,6 +213,9 @@ int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t 
 int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
                 uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 
+// symmetric SQ8 encoding of n x 100 device rows with a given alpha (sq8.cu)
+void launch_sq8_encode(const float *d_x, uint64_t n, float alpha, int8_t *d_codes, cudaStream_t st);
+
 // launch counter (kernels launched by this library in the current call)
 extern thread_local uint32_t g_launches;
 

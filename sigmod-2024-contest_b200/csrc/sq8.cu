@@ -49,24 +49,6 @@ __global__ void k_sq8_encode(const float *__restrict__ x, uint64_t n, float alph
   }
 }
 
-__device__ __forceinline__ int sq8_dist(const int *__restrict__ qw, int qq, const int8_t *__restrict__ code) {
-  const int4 *c4 = reinterpret_cast<const int4 *>(code);
-  int cc = 0, qc = 0;
-#pragma unroll
-  for (int w = 0; w < SQ8_WORDS / 4; ++w) {
-    const int4 v = c4[w];
-    cc = __dp4a(v.x, v.x, cc);
-    cc = __dp4a(v.y, v.y, cc);
-    cc = __dp4a(v.z, v.z, cc);
-    cc = __dp4a(v.w, v.w, cc);
-    qc = __dp4a(qw[4 * w + 0], v.x, qc);
-    qc = __dp4a(qw[4 * w + 1], v.y, qc);
-    qc = __dp4a(qw[4 * w + 2], v.z, qc);
-    qc = __dp4a(qw[4 * w + 3], v.w, qc);
-  }
-  return qq + cc - 2 * qc;
-}
-
 struct HeapNode {
   int d;
   int id;
@@ -290,6 +272,12 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
 }
 
 }  // namespace
+
+void launch_sq8_encode(const float *d_x, uint64_t n, float alpha, int8_t *d_codes, cudaStream_t st) {
+  k_sq8_encode<<<148 * 8, 256, 0, st>>>(d_x, n, alpha, d_codes);
+  g_launches += 1;
+}
+
 }  // namespace fknn
 
 using namespace fknn;

@@ -26,6 +26,14 @@ MODE_EXACT_FP32 = 0
 MODE_BF16_RERANK = 1
 MODE_FP8_RERANK = 2
 
+# Graph search forms (include/fknn.h FKNN_GRAPH_*), numbered as the Searcher methods.
+GRAPH_SEARCH = 0
+GRAPH_FILTER = 1
+GRAPH_FILTER_SUBTIME = 2
+GRAPH_CATEGORY_RANGE = 3
+GRAPH_RANGE_SUBTIME = 4
+GRAPH_RANGE = 5
+
 _ERRNAMES = {
     FKNN_EINVAL: "FKNN_EINVAL",
     FKNN_ENOMEM: "FKNN_ENOMEM",
@@ -92,6 +100,11 @@ SIGNATURES = {
     "fknn_sq8_bruteforce": (c_int, [c_size_t, c_size_t, c_void_p, c_size_t, c_void_p, c_float, c_size_t, c_void_p]),
     "fknn_sq8_bruteforce_subgraph": (c_int, [c_size_t, c_size_t, c_void_p, c_void_p, c_size_t, c_void_p, c_float,
                                              c_size_t, c_void_p]),
+    "fknn_graph_create": (c_int, [c_void_p, c_size_t, c_void_p, c_int, POINTER(c_void_p)]),
+    "fknn_graph_destroy": (c_int, [c_void_p]),
+    "fknn_graph_info": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_float)]),
+    "fknn_graph_search": (c_int, [c_void_p, c_void_p, c_uint32, c_int, c_uint32, c_uint32, c_uint32, c_void_p,
+                                  c_void_p, c_void_p, c_void_p, c_void_p]),
 }
 
 _lib = None

@@ -5,6 +5,9 @@ Reference interfaces mirrored (paths inside KevinZeng08/sigmod-2024-contest):
   bruteforce(dim, k, closest_points, npoints, ...)    bruteforce.h:244-265
   bruteforce_subgraph(..., distances, ...)            bruteforce.h:267-289
   SQ8SymmetricQuantizer.train / encode                pyglass/glass/quant/sq8_sym_quant.hpp:32-74
+  GraphSearcher: Graph::load + Searcher::SetData and the six Search* forms
+                                                      pyglass/glass/graph.hpp:117-137,
+                                                      pyglass/glass/searcher.hpp:94-101,162-569
 plus the resident-index form (Index) that the batch path uses.
 
 Arrays may be numpy (host) or torch tensors (host or CUDA); torch CUDA tensors
@@ -13,7 +16,7 @@ are passed to the library as device pointers and stay on the device.
 from __future__ import annotations
 
 import ctypes
-from ctypes import byref, c_float, c_uint64, c_void_p
+from ctypes import byref, c_float, c_uint32, c_uint64, c_void_p
 from typing import Optional, Sequence
 
 import numpy as np
@@ -214,3 +217,102 @@ def bruteforce_subgraph(dim: int, k: int, closest_points, distances, npoints: in
     check(load().fknn_sq8_bruteforce_subgraph(dim, k, _ptr(closest_points, np.int32), _ptr(distances, np.float32),
                                               npoints, _ptr(codes_in, np.int8), c_float(alpha), nqueries,
                                               _ptr(queries_in, np.int8)))
+
+
+class GraphSearcher:
+    """The pyglass Searcher over one saved graph (Graph::save bytes), batched.
+
+    Method names and arguments follow searcher.hpp; each takes a batch of
+    queries (nq x 100) and returns ids (nq x refine, int32) -- and distances
+    for the *SubTime forms -- equal to the reference's on the same graph.
+    ``k`` is the reference's pool argument (capacity max(k, ef)).
+    """
+
+    def __init__(self, graph_bytes, data, device: int = 0):
+        lib = load()
+        gb = np.frombuffer(bytes(graph_bytes), dtype=np.uint8) if not isinstance(graph_bytes, np.ndarray) \
+            else np.ascontiguousarray(graph_bytes, dtype=np.uint8)
+        if _is_torch(data) and data.is_cuda:
+            d = data
+        else:
+            d = np.ascontiguousarray(data, dtype=np.float32).reshape(-1, DIM)
+        h = c_void_p()
+        check(lib.fknn_graph_create(gb.ctypes.data, gb.size, _ptr(d, np.float32), device, byref(h)))
+        self._h = h
+        self.ef = 32
+        n, deg, a = c_uint32(), c_uint32(), c_float()
+        check(lib.fknn_graph_info(self._h, byref(n), byref(deg), byref(a)))
+        self.nb, self.degree, self.alpha = n.value, deg.value, a.value
+
+    @classmethod
+    def load(cls, path: str, data, device: int = 0) -> "GraphSearcher":
+        with open(path, "rb") as f:
+            return cls(f.read(), data, device)
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().fknn_graph_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def SetEf(self, ef: int) -> None:
+        self.ef = int(ef)
+
+    def _run(self, mode, q, k, refine, bounds=None, id_bounds=None, with_dists=False, stream=None):
+        lib = load()
+        dev = _is_torch(q) and q.is_cuda
+        if dev:
+            import torch
+            nq = q.shape[0]
+            ids = torch.empty((nq, refine), dtype=torch.int32, device=q.device)
+            dists = torch.empty((nq, refine), dtype=torch.float32, device=q.device) if with_dists else None
+            if stream is None:
+                stream = _stream_of(q)
+        else:
+            q = np.ascontiguousarray(q, dtype=np.float32).reshape(-1, DIM)
+            nq = q.shape[0]
+            ids = np.empty((nq, refine), dtype=np.int32)
+            dists = np.empty((nq, refine), dtype=np.float32) if with_dists else None
+        if bounds is not None and not _is_torch(bounds):
+            bounds = np.ascontiguousarray(bounds, dtype=np.float32).reshape(nq, 2)
+        if id_bounds is not None and not _is_torch(id_bounds):
+            id_bounds = np.ascontiguousarray(id_bounds, dtype=np.int32).reshape(nq, 2)
+        check(lib.fknn_graph_search(self._h, _ptr(q, np.float32), nq, mode, k, self.ef, refine,
+                                    _ptr(bounds, np.float32), _ptr(id_bounds, np.int32), _ptr(ids, np.int32),
+                                    _ptr(dists, np.float32) if dists is not None else None, stream))
+        return (ids, dists) if with_dists else ids
+
+    def Search(self, q, k: int):
+        """searcher.hpp:162: k ids per query."""
+        return self._run(_lib.GRAPH_SEARCH, q, k, k)
+
+    def SearchFilter(self, q, k: int, refine: int):
+        """searcher.hpp:262 (the filter argument is unused by the reference)."""
+        return self._run(_lib.GRAPH_FILTER, q, k, refine)
+
+    def SearchFilterSubTime(self, q, k: int, refine: int):
+        """searcher.hpp:377: (ids, dists)."""
+        return self._run(_lib.GRAPH_FILTER_SUBTIME, q, k, refine, with_dists=True)
+
+    def SearchCategoryRange(self, q, k: int, refine: int, query_bound, id_bound):
+        """searcher.hpp:301: per query (l, r) and (s_id, e_id)."""
+        return self._run(_lib.GRAPH_CATEGORY_RANGE, q, k, refine, query_bound, id_bound)
+
+    def SearchRangeFilterSubTime(self, q, k: int, refine: int, query_bound, id_bound):
+        """searcher.hpp:415: (ids, dists)."""
+        return self._run(_lib.GRAPH_RANGE_SUBTIME, q, k, refine, query_bound, id_bound, with_dists=True)
+
+    def SearchRangeFilter(self, q, k: int, refine: int, query_bound, id_bound):
+        """searcher.hpp:493."""
+        return self._run(_lib.GRAPH_RANGE, q, k, refine, query_bound, id_bound)

@@ -20,6 +20,10 @@ Fixtures (all small):
   sq8_kat.json     the known answer of test_simd_distance.cpp:196-203: the
                    two fixed int8 vectors parsed from that file and the
                    reference L2SqrSQ8_sym value
+  graph_hnsw.npz   a graph built by the reference HNSW::Build (Graph::save
+                   bytes, N=2000, R=24, points in timestamp order) and the
+                   reference Searcher's ids (and dists) for all six search
+                   forms over seeded queries, time windows and id ranges
 Each npz also stores the SHA-256 of the generated inputs so a generator
 change is detected instead of silently compared.
 """
@@ -38,8 +42,10 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
 sys.path.insert(0, os.path.join(ROOT, "oracle"))
 sys.path.insert(0, os.path.join(ROOT, "sigmod-2024-contest_b200"))
+sys.path.insert(0, os.path.dirname(HERE))
 import oracle  # noqa: E402
 from fknn import datagen  # noqa: E402
+from graph_util import GRAPH_CASES, graph_inputs  # noqa: E402
 
 REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
 
@@ -153,11 +159,27 @@ def sq8_kat():
     print("sq8_kat.json", val)
 
 
+def graph_case():
+    vecs, labels, ts, q, bounds, ib = graph_inputs()
+    path = "/tmp/fknn_golden_graph.bin"
+    gb = oracle.ref_hnsw_graph(vecs, ts, 24, 100, path)
+    out = {}
+    for j, (mode, k, refine) in enumerate(GRAPH_CASES):
+        wd = mode in (2, 4)
+        r = oracle.ref_graph_search(path, vecs, labels, ts, q, mode, k, refine, bounds, ib, with_dists=wd)
+        out[f"ids{j}"] = r[0] if wd else r
+        if wd:
+            out[f"dists{j}"] = r[1]
+    np.savez_compressed(os.path.join(HERE, "graph_hnsw.npz"), graph=np.frombuffer(gb, dtype=np.uint8),
+                        cases=np.array(GRAPH_CASES, dtype=np.int32), bounds=bounds, id_bounds=ib,
+                        sha_inputs=digest(vecs, labels, ts, q), **out)
+    print("graph_hnsw.npz", len(gb), "graph bytes")
+
+
+CASES = {"exact": lambda: (exact_case("exact_c1.npz", 1, 20000, 300), exact_case("exact_c4.npz", 4, 20000, 200)),
+         "ties": ties_case, "dummy": dummy_case, "sq8": sq8_case, "kat": sq8_kat, "graph": graph_case}
+
 if __name__ == "__main__":
     oracle.build(ref=True)
-    exact_case("exact_c1.npz", 1, 20000, 300)
-    exact_case("exact_c4.npz", 4, 20000, 200)
-    ties_case()
-    dummy_case()
-    sq8_case()
-    sq8_kat()
+    for name in (sys.argv[1:] or list(CASES)):
+        CASES[name]()

@@ -143,3 +143,64 @@ def test_sq8_restatement_equals_live_reference():
         ids = np.empty(k, dtype=np.int32)
         R.ref_sq8_bruteforce(k, ids.ctypes.data, 3000, codes.ctypes.data, ctypes.c_float(1.0), qv.ctypes.data)
         np.testing.assert_array_equal(oracle.sq8_bruteforce(k, codes, 1.0, qv), ids)
+
+
+def _graph_fixture(golden_dir):
+    from graph_util import graph_inputs
+    f = np.load(os.path.join(golden_dir, "graph_hnsw.npz"))
+    vecs, labels, ts, q, bounds, ib = graph_inputs()
+    assert _digest(vecs, labels, ts, q) == str(f["sha_inputs"]), "generator output changed"
+    np.testing.assert_array_equal(bounds, f["bounds"])
+    np.testing.assert_array_equal(ib, f["id_bounds"])
+    return f, vecs, labels, ts, q, bounds, ib
+
+
+def test_graph_search_matches_reference_fixture(golden_dir):
+    """Restated Searcher == the reference Searcher on a reference HNSW graph,
+    all six search forms (searcher.hpp:162-569)."""
+    f, vecs, labels, ts, q, bounds, ib = _graph_fixture(golden_dir)
+    gb = f["graph"].tobytes()
+    for j, (mode, k, refine) in enumerate(f["cases"]):
+        wd = int(mode) in (2, 4)
+        out = oracle.graph_search(gb, vecs, q, int(mode), int(k), int(refine), bounds, ib, with_dists=wd)
+        ids = out[0] if wd else out
+        np.testing.assert_array_equal(ids, f[f"ids{j}"], err_msg=f"case {j} mode {mode}")
+        if wd:
+            np.testing.assert_array_equal(out[1], f[f"dists{j}"], err_msg=f"case {j} mode {mode}")
+
+
+def test_graph_search_rejects_bad_inputs():
+    from graph_util import random_graph
+    ts = np.sort(np.random.default_rng(1).random(500).astype(np.float32))
+    gb = random_graph(500, 16, ts, seed=3)
+    vecs = np.random.default_rng(2).standard_normal((500, 100)).astype(np.float32)
+    with pytest.raises(ValueError):  # truncated bytes
+        oracle.graph_search(gb[:-7], vecs, vecs[:2], 0, 10, 10)
+    with pytest.raises(ValueError):  # a seed past the last point
+        oracle.graph_search(gb, vecs, vecs[:1], 3, 10, 10, np.array([[0, 1]], np.float32),
+                            np.array([[600, 700]], np.int32))
+
+
+@pytest.mark.skipif(oracle.ref_graph() is None, reason="reference graph objects not built (oracle/_ref)")
+def test_graph_restatement_equals_live_reference(tmp_path):
+    """Seeded HNSW graphs of several sizes and degrees; the restated Searcher
+    equals the reference Searcher call for call."""
+    from graph_util import id_bounds_for, windows
+    for (n, R, cfg) in [(3000, 16, 1), (12000, 32, 4)]:
+        vecs, labels, ts, q, metas = datagen.make_workload(cfg, n=n, nq=40)
+        order = np.argsort(ts, kind="stable")
+        vecs, labels, ts = vecs[order], labels[order], ts[order]
+        path = str(tmp_path / f"g{n}.bin")
+        gb = oracle.ref_hnsw_graph(vecs, ts, R, 80, path)
+        bounds = windows(q.shape[0], n, log_w=(-4, 0))
+        ib = id_bounds_for(ts, bounds)
+        for mode, k, refine in [(0, 50, 50), (1, 500, 150), (2, 120, 60), (3, 200, 150), (4, 200, 150),
+                                (5, 33, 34)]:
+            wd = mode in (2, 4)
+            r = oracle.ref_graph_search(path, vecs, labels, ts, q, mode, k, refine, bounds, ib, with_dists=wd)
+            o = oracle.graph_search(gb, vecs, q, mode, k, refine, bounds, ib, with_dists=wd)
+            if wd:
+                np.testing.assert_array_equal(o[0], r[0])
+                np.testing.assert_array_equal(o[1], r[1])
+            else:
+                np.testing.assert_array_equal(o, r)
