@@ -53,6 +53,11 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="queries in the CPU-baseline sample")
     ap.add_argument("--kprime", type=int, default=200, help="candidate width of the BF16 form")
+    ap.add_argument("--sweep", action="store_true",
+                    help="precision sweep instead of the headline: exact, BF16 and FP8 forms at k' in "
+                         "--kprimes, recall and distance error against an FP64 oracle sample; one JSON line each")
+    ap.add_argument("--kprimes", default="200,400,800")
+    ap.add_argument("--f64-sample", type=int, default=128, help="queries checked against the FP64 oracle")
     return ap.parse_args()
 
 
@@ -227,8 +232,79 @@ def run_reference(args, rank: int, world: int):
     print(json.dumps(line), flush=True)
 
 
+def run_sweep(args):
+    """Per form and k': queries/s (inputs resident), recall@100 against the
+    exact GPU path over all queries and against the FP64 oracle on a seeded
+    sample, and the distance error against FP64: max relative error of the
+    returned distances (FP64 recomputed for the same ids) and of the k-th
+    distance (against the FP64 oracle's k-th)."""
+    import torch
+
+    import fknn
+    import oracle
+    from fknn import datagen
+    torch.cuda.set_device(0)
+    w = datagen.WORKLOADS[args.config]
+    n, nq = args.n or w.n, args.nq or w.nq
+    vecs, labels, ts, q, metas = datagen.make_workload(args.config, n=n, nq=nq)
+    idx = fknn.Index(vecs, labels, ts, build_bf16=True, build_fp8=True)
+    stream = torch.cuda.current_stream()
+    dq, dm = torch.from_numpy(q).cuda(), torch.from_numpy(metas).cuda()
+    rng = np.random.default_rng(17)
+    sel = np.sort(rng.choice(nq, size=min(args.f64_sample, nq), replace=False))
+    t0 = time.perf_counter()
+    o_ids, o_d = oracle.exact_knn(vecs, labels, ts, q[sel], metas[sel], f64=True)
+    t_oracle = time.perf_counter() - t0
+
+    def run(mode, kprime):
+        ids = torch.empty((nq, 100), dtype=torch.int32, device="cuda")
+        dd = torch.empty((nq, 100), dtype=torch.float32, device="cuda")
+        for _ in range(args.warmup):
+            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / args.steps, ids.cpu().numpy().view(np.uint32).copy(), dd.cpu().numpy()
+
+    def errors(ids, dd):
+        s_ids, s_d = ids[sel], dd[sel]
+        valid = s_ids != 0xFFFFFFFF
+        x = vecs[np.where(valid, s_ids, 0)].astype(np.float64)
+        d64 = ((x - q[sel][:, None, :].astype(np.float64)) ** 2).sum(-1)
+        rel = np.abs(s_d.astype(np.float64) - d64) / np.maximum(d64, 1e-30)
+        o_valid = o_ids != 0xFFFFFFFF
+        kth = []
+        for i in range(len(sel)):
+            m = int(min(valid[i].sum(), o_valid[i].sum()))
+            if m:
+                kth.append(abs(float(s_d[i, m - 1]) - float(o_d[i, m - 1])) / max(float(o_d[i, m - 1]), 1e-30))
+        return {"recall_at_100_vs_f64_oracle": datagen.recall_matrix(s_ids, o_ids),
+                "max_rel_dist_error_returned": float(rel[valid].max()) if valid.any() else 0.0,
+                "max_rel_kth_dist_error": max(kth) if kth else 0.0}
+
+    ms_e, ids_e, d_e = run(fknn.MODE_EXACT_FP32, 0)
+    base = {"config": {"workload": w.name, "n": n, "nq": nq, "k": 100, "d": 100},
+            "f64_sample": {"queries": int(len(sel)), "oracle_seconds": t_oracle}}
+    print(json.dumps({**base, "form": "exact_fp32", "kprime": None, "value": nq / (ms_e * 1e-3), "unit": UNIT,
+                      "ms_per_step": ms_e, "recall_at_100_vs_exact_gpu": 1.0, **errors(ids_e, d_e)}), flush=True)
+    for mode, name in ((fknn.MODE_BF16_RERANK, "bf16_rerank"), (fknn.MODE_FP8_RERANK, "fp8_rerank")):
+        for kp in [int(x) for x in args.kprimes.split(",")]:
+            ms, ids, dd = run(mode, kp)
+            print(json.dumps({**base, "form": name, "kprime": kp, "value": nq / (ms * 1e-3), "unit": UNIT,
+                              "ms_per_step": ms, "speedup_vs_exact": ms_e / ms,
+                              "recall_at_100_vs_exact_gpu": datagen.recall_matrix(ids, ids_e),
+                              **errors(ids, dd)}), flush=True)
+    idx.close()
+
+
 def main():
     args = parse()
+    if args.sweep:
+        return run_sweep(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
