@@ -58,6 +58,12 @@ def parse():
                          "--kprimes, recall and distance error against an FP64 oracle sample; one JSON line each")
     ap.add_argument("--kprimes", default="200,400,800")
     ap.add_argument("--f64-sample", type=int, default=128, help="queries checked against the FP64 oracle")
+    ap.add_argument("--serve", action="store_true",
+                    help="request-loop run instead of the headline: Poisson arrivals at --rates per form; "
+                         "one JSON line per (form, rate)")
+    ap.add_argument("--rates", default="10000,50000,200000")
+    ap.add_argument("--serve-seconds", type=float, default=2.0)
+    ap.add_argument("--serve-forms", default="bf16,exact")
     return ap.parse_args()
 
 
@@ -301,10 +307,75 @@ def run_sweep(args):
     idx.close()
 
 
+def run_serve(args):
+    """The request loop (fknn.Server) under Poisson arrivals: for each form
+    and rate, requests (one query each, config-4/5 generator) arrive for
+    --serve-seconds; a client thread submits each due request with its
+    arrival stamp, so queueing before submission counts as latency.  Reports
+    p50/p99 latency (arrival -> result), sustained queries/s (results / first
+    arrival to last result) and recall@100 of the served ids against the
+    exact path's ids for the same queries."""
+    import torch
+
+    import fknn
+    from fknn import datagen
+    torch.cuda.set_device(0)
+    cfg = 5 if args.config == 2 else args.config
+    w = datagen.WORKLOADS[cfg]
+    n = args.n or w.n
+    rates = [int(x) for x in args.rates.split(",")]
+    nreq = int(max(rates) * args.serve_seconds) + 1
+    vecs, labels, ts, q, metas = datagen.make_workload(cfg, n=n, nq=nreq)
+    idx = fknn.Index(vecs, labels, ts, build_bf16=True)
+    exact_ids, _ = idx.search(q, metas, k=100, mode=fknn.MODE_EXACT_FP32)
+    forms = {"bf16": (fknn.MODE_BF16_RERANK, args.kprime), "exact": (fknn.MODE_EXACT_FP32, 0)}
+    for fname in args.serve_forms.split(","):
+        mode, kp = forms[fname]
+        with fknn.Server(idx, mode=mode, kprime=kp, max_batch=4096, slots=3) as srv:
+            # size every slot's scratch for a full batch of each query type first
+            for t in range(4):
+                sel = np.nonzero(metas[:, 0] == t)[0][:4096]
+                for _ in range(3):
+                    srv.submit(q[sel], metas[sel], with_dists=False)
+            srv.drain()
+            srv.stats(reset=True)
+            for rate in rates:
+                m = int(rate * args.serve_seconds)
+                rng = np.random.default_rng(rate)
+                arr = np.cumsum(rng.exponential(1e9 / rate, m)).astype(np.int64)
+                ids = np.empty((m, 100), dtype=np.uint32)
+                t0 = srv.now_ns() + 1_000_000
+                arr += t0
+                i = 0
+                while i < m:
+                    now = srv.now_ns()
+                    j = int(np.searchsorted(arr, now, side="right"))
+                    if j > i:
+                        srv.submit(q[i:j], metas[i:j], arrival_ns=arr[i:j], with_dists=False, ids=ids[i:j])
+                        i = j
+                    else:
+                        time.sleep(max(0.0, min(2e-4, (arr[i] - now) * 1e-9)))
+                srv.drain()
+                st = srv.stats(reset=True)
+                rec = datagen.recall_matrix(ids, exact_ids[:m].view(np.uint32))
+                print(json.dumps({
+                    "mode": "serve", "form": fname, "kprime": kp or None,
+                    "config": {"workload": w.name, "n": n, "k": 100, "d": 100, "arrivals": "poisson",
+                               "offered_qps": rate, "seconds": args.serve_seconds, "requests": m,
+                               "max_batch": 4096, "slots": 3},
+                    "sustained_qps": st["qps"], "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+                    "max_ms": st["max_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"],
+                    "admission_waits": st["admission_waits"], "budget_trims": st["budget_trims"],
+                    "scratch_bytes": st["scratch_bytes"], "recall_at_100_vs_exact": rec}), flush=True)
+    idx.close()
+
+
 def main():
     args = parse()
     if args.sweep:
         return run_sweep(args)
+    if args.serve:
+        return run_serve(args)
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))

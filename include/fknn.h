@@ -211,6 +211,67 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
                       uint32_t refine, const float *bounds, const int32_t *id_bounds, int32_t *out_ids,
                       float *out_dists, void *stream);
 
+/* ---- Request loop (continuous batching over one resident index) ----
+ *
+ * No reference counterpart: the reference answers one offline batch
+ * (baseline.cpp:150 -> HybridGraph::BatchSearch).  Requests (one query
+ * each) are queued per query type; whenever one of `slots` search slots is
+ * free, the oldest type's waiting requests -- up to max_batch -- are
+ * searched together on that slot's stream while the other slots' batches
+ * run.  A batch starts only while the device scratch the slots hold fits in
+ * hbm_budget; a batch that runs over it releases its slot's scratch and
+ * lowers the batch size for its query type.  Each result equals what
+ * fknn_search returns for that query alone. */
+
+typedef struct fknn_server fknn_server;
+
+typedef struct fknn_server_opts {
+  int mode;              /* FKNN_MODE_* for every request */
+  uint32_t kprime;       /* candidate width of the reduced-precision modes (0 = default) */
+  uint32_t k;            /* neighbours per request, <= 128 (0 = 100) */
+  uint32_t max_batch;    /* queries per batch (0 = 4096) */
+  uint32_t slots;        /* batches in flight (0 = 3, max 16) */
+  uint32_t max_wait_us;  /* a partial batch may wait this long for more requests while other
+                            slots keep the device busy (0 = dispatch at once) */
+  uint64_t hbm_budget;   /* device bytes the slots' scratch may hold (0 = half the free HBM) */
+} fknn_server_opts;
+
+typedef struct fknn_server_stats {
+  uint64_t submitted, completed, failed, batches;
+  uint64_t admission_waits; /* times a free slot waited because the held scratch exceeded the budget */
+  uint64_t budget_trims;    /* batches that ran over the budget (their slot released its scratch and
+                               the type's batch size was lowered) */
+  uint64_t scratch_bytes;   /* device bytes held by the slots' scratch */
+  uint64_t budget_bytes;
+  uint32_t max_batch_seen;
+  float mean_batch;
+  float p50_ms, p99_ms, max_ms, mean_ms; /* arrival -> result, requests completed since the last reset */
+  double span_s;            /* first arrival -> last result of those requests */
+  double qps;               /* their count / span_s */
+} fknn_server_stats;
+
+/* The index must outlive the server.  The server holds one search view of
+ * the index per slot; direct fknn_search calls on the index stay valid. */
+int fknn_server_create(fknn_index *index, const fknn_server_opts *opts, fknn_server **out);
+/* The clock arrival stamps are read against (steady, nanoseconds). */
+int64_t fknn_server_now_ns(void);
+/* Enqueues nreq requests: qvecs nreq x 100 and metas nreq x 4 (type, v, l,
+ * r) host memory, copied before returning; arrival_ns (nullable = now) the
+ * time each request arrived, from which its latency counts.  ids (nreq x k)
+ * and dists (nullable, nreq x k) are host memory written when each request
+ * completes and must stay valid until then.  Tickets are first_ticket ..
+ * first_ticket + nreq - 1.  A request that fails validation rejects the call
+ * (nothing is enqueued). */
+int fknn_server_submit(fknn_server *s, const float *qvecs, const float *metas, uint32_t nreq,
+                       const int64_t *arrival_ns, uint32_t *ids, float *dists, uint64_t *first_ticket);
+/* Waits for one request (timeout_ms < 0: forever); returns its status. */
+int fknn_server_wait(fknn_server *s, uint64_t ticket, int timeout_ms);
+/* Waits for every submitted request; returns the first failure's status. */
+int fknn_server_drain(fknn_server *s, int timeout_ms);
+int fknn_server_get_stats(fknn_server *s, fknn_server_stats *out, int reset);
+/* Drains, then stops the threads and frees the slots. */
+int fknn_server_destroy(fknn_server *s);
+
 #ifdef __cplusplus
 }
 #endif

@@ -846,14 +846,11 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
     else
       k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), d_desc, (__nv_bfloat16 *)d_at,
                                                d_lqs);
-    static bool attr = false;
-    if (!attr) {
-      FKNN_CUDA(cudaFuncSetAttribute(k_screen_tc<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(BScreenSmem<F>)));
-      FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)sizeof(RerankSmem)));
-      attr = true;
-    }
+    // per device context, so set on every call (cheap)
+    FKNN_CUDA(cudaFuncSetAttribute(k_screen_tc<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(BScreenSmem<F>)));
+    FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(RerankSmem)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
     void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
     k_screen_tc<F><<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(

@@ -88,6 +88,14 @@ static void free_index(fknn_index *idx) {
   if (!idx) return;
   cudaSetDevice(idx->device);
   cudaDeviceSynchronize();
+  if (idx->is_view) {
+    for (auto &b : idx->ws) cudaFree(b.p);
+    for (auto &b : idx->hs)
+      if (b.p) cudaFreeHost(b.p);
+    cudaFree(idx->d_flag);
+    delete idx;
+    return;
+  }
   cudaFree(idx->vecs);
   cudaFree(idx->norms);
   cudaFree(idx->labels_f);
@@ -107,6 +115,55 @@ static void free_index(fknn_index *idx) {
   cudaFree(idx->d_flag);
   if (idx->own_stream) cudaStreamDestroy(idx->own_stream);
   delete idx;
+}
+
+int make_index_view(fknn_index *base, fknn_index **out) {
+  *out = nullptr;
+  fknn_index *v = new (std::nothrow) fknn_index();
+  if (!v) {
+    set_error("out of host memory");
+    return FKNN_ENOMEM;
+  }
+  v->device = base->device;
+  v->n = base->n;
+  v->nblk = base->nblk;
+  v->vecs = base->vecs;
+  v->norms = base->norms;
+  v->labels_f = base->labels_f;
+  v->ts_f = base->ts_f;
+  for (int o = 0; o < 2; ++o) {
+    v->ord[o] = base->ord[o];
+    v->bf16_blocks[o] = base->bf16_blocks[o];
+    v->fp8_blocks[o] = base->fp8_blocks[o];
+  }
+  v->fp8_scale = base->fp8_scale;
+  v->is_view = true;
+  cudaError_t e = cudaSetDevice(v->device);
+  if (e == cudaSuccess) e = cudaMalloc(&v->d_flag, 64);
+  if (e != cudaSuccess) {
+    delete v;
+    return cuda_fail(e, "cudaMalloc");
+  }
+  *out = v;
+  return FKNN_OK;
+}
+
+void destroy_index(fknn_index *idx) { free_index(idx); }
+
+void trim_scratch(fknn_index *idx) {
+  std::lock_guard<std::mutex> lock(idx->mu);
+  cudaSetDevice(idx->device);
+  for (auto &w : idx->ws) {
+    dev_free(idx, w.p, w.bytes);
+    w.p = nullptr;
+    w.bytes = 0;
+  }
+}
+
+uint64_t scratch_bytes(const fknn_index *idx) {
+  uint64_t b = 0;
+  for (const auto &w : idx->ws) b += w.bytes;
+  return b;
 }
 
 }  // namespace fknn
@@ -275,9 +332,9 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
   if (rc) return rc;
   if (!i_dev) FKNN_CUDA(cudaMemcpyAsync(ids, d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && !dd_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_dists, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
-  FKNN_CUDA(cudaStreamSynchronize(st));
   int flag = 0;
-  FKNN_CUDA(cudaMemcpy(&flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost));
+  FKNN_CUDA(cudaMemcpyAsync(&flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
   if (flag & (1 << 8)) {
     set_error("fknn_search: a bounded device wait gave up; affected queries were answered by the exact scan");
   }

@@ -1024,12 +1024,9 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
     if ((rc = ws_get(idx, 7, (size_t)nitems * TQ * 4, (void **)&d_ocnt))) return rc;
     k_tile_stage<<<ntile, 256, 0, st>>>(d_q, d_desc, (const int32_t *)(d_blob + o_lq), d_qt);
     const size_t smem = sizeof(ScreenSmem);
-    static bool attr_set = false;
-    if (!attr_set) {
-      FKNN_CUDA(cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-      FKNN_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MergeSmem)));
-      attr_set = true;
-    }
+    // per device context, so set on every call (cheap)
+    FKNN_CUDA(cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    FKNN_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MergeSmem)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
     k_screen<<<nitems, SC_THREADS, smem, st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_qt, (const int32_t *)(d_blob + o_lq),

@@ -171,6 +171,9 @@ struct fknn_index {
   fknn::HostBuf hs[8];
   int *d_flag = nullptr;
   cudaStream_t own_stream = nullptr;
+  // a view shares the device data of another index and owns only its
+  // per-call scratch (ws, hs, d_flag), so views search concurrently
+  bool is_view = false;
 };
 
 namespace fknn {
@@ -185,6 +188,11 @@ int cuda_fail(cudaError_t e, const char *what);
   } while (0)
 
 int dev_alloc(fknn_index *idx, void **p, size_t bytes);
+// search views of one index (capi.cu)
+int make_index_view(fknn_index *base, fknn_index **out);
+void destroy_index(fknn_index *idx);
+uint64_t scratch_bytes(const fknn_index *idx);
+void trim_scratch(fknn_index *idx);
 int ws_get(fknn_index *idx, int slot, size_t bytes, void **p);
 int hs_get(fknn_index *idx, int slot, size_t bytes, void **p);
 

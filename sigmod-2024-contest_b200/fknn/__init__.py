@@ -6,11 +6,11 @@ the reference's entry points (see api.py).
 """
 from ._lib import (FKNN_EINVAL, FKNN_ENOMEM, FKNN_EUNSUPPORTED, FKNN_OK, MODE_BF16_RERANK, MODE_EXACT_FP32,
                    MODE_FP8_RERANK, FknnError, LIB_PATH, load)
-from .api import (DIM, K, Bruteforce, GraphSearcher, Index, SQ8SymmetricQuantizer, bruteforce,
+from .api import (DIM, K, Bruteforce, GraphSearcher, Index, Server, SQ8SymmetricQuantizer, bruteforce,
                   bruteforce_subgraph)
 
 __all__ = [
-    "Index", "GraphSearcher", "Bruteforce", "bruteforce", "bruteforce_subgraph", "SQ8SymmetricQuantizer", "FknnError", "load",
+    "Index", "GraphSearcher", "Server", "Bruteforce", "bruteforce", "bruteforce_subgraph", "SQ8SymmetricQuantizer", "FknnError", "load",
     "LIB_PATH", "DIM", "K", "MODE_EXACT_FP32", "MODE_BF16_RERANK", "MODE_FP8_RERANK", "FKNN_OK", "FKNN_EINVAL",
     "FKNN_ENOMEM", "FKNN_EUNSUPPORTED",
 ]

@@ -79,6 +79,35 @@ class SearchStats(Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class ServerOpts(Structure):
+    _fields_ = [("mode", c_int), ("kprime", c_uint32), ("k", c_uint32), ("max_batch", c_uint32),
+                ("slots", c_uint32), ("max_wait_us", c_uint32), ("hbm_budget", c_uint64)]
+
+
+class ServerStats(Structure):
+    _fields_ = [
+        ("submitted", c_uint64),
+        ("completed", c_uint64),
+        ("failed", c_uint64),
+        ("batches", c_uint64),
+        ("admission_waits", c_uint64),
+        ("budget_trims", c_uint64),
+        ("scratch_bytes", c_uint64),
+        ("budget_bytes", c_uint64),
+        ("max_batch_seen", c_uint32),
+        ("mean_batch", c_float),
+        ("p50_ms", c_float),
+        ("p99_ms", c_float),
+        ("max_ms", c_float),
+        ("mean_ms", c_float),
+        ("span_s", ctypes.c_double),
+        ("qps", ctypes.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # Every entry point of include/fknn.h with its ctypes signature.
 SIGNATURES = {
     "fknn_version": (c_int, []),
@@ -105,6 +134,14 @@ SIGNATURES = {
     "fknn_graph_info": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_float)]),
     "fknn_graph_search": (c_int, [c_void_p, c_void_p, c_uint32, c_int, c_uint32, c_uint32, c_uint32, c_void_p,
                                   c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fknn_server_create": (c_int, [c_void_p, POINTER(ServerOpts), POINTER(c_void_p)]),
+    "fknn_server_now_ns": (ctypes.c_int64, []),
+    "fknn_server_submit": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p,
+                                   POINTER(c_uint64)]),
+    "fknn_server_wait": (c_int, [c_void_p, c_uint64, c_int]),
+    "fknn_server_drain": (c_int, [c_void_p, c_int]),
+    "fknn_server_get_stats": (c_int, [c_void_p, POINTER(ServerStats), c_int]),
+    "fknn_server_destroy": (c_int, [c_void_p]),
 }
 
 _lib = None
