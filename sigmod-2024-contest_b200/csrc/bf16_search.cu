@@ -300,87 +300,113 @@ struct BScreenSmem {
   uint32_t tmem_base;
 };
 
-// kth smallest screening distance of a list (warp radix select over the
-// order-preserving integer image; 4 passes of 8 bits).
-__device__ float warp_select_kth(const Candidate *list, int n, int kth, uint32_t *hist) {
+// kth smallest (1-based) of the n keys held NPL per lane (element
+// j*32 + lane in key[j]; keys past n ignored): a warp radix select that
+// starts below the bits all keys share and takes up to 8 bits per pass from
+// a shared-memory histogram.  Keys are order-preserving images of floats.
+template <int NPL>
+__device__ __forceinline__ uint32_t warp_kth_regs(const uint32_t (&key)[NPL], int n, int kth, uint32_t *hist) {
   const int lane = threadIdx.x & 31;
-  uint32_t prefix = 0, mask = 0;
-  int remaining = kth;
-  for (int pass = 0; pass < 4; ++pass) {
-    const int shift = 24 - 8 * pass;
-    for (int i = lane; i < 256; i += 32) hist[i] = 0;
-    __syncwarp();
-    for (int i = lane; i < n; i += 32) {
-      const uint32_t u = f32_sortable(list[i].ds);
-      if ((u & mask) == prefix) atomicAdd(&hist[(u >> shift) & 255], 1u);
+  uint32_t mn = 0xffffffffu, mx = 0u;
+#pragma unroll
+  for (int j = 0; j < NPL; ++j)
+    if (j * 32 + lane < n) {
+      mn = min(mn, key[j]);
+      mx = max(mx, key[j]);
     }
+  mn = __reduce_min_sync(0xffffffffu, mn);
+  mx = __reduce_max_sync(0xffffffffu, mx);
+  if (mn == mx) return mn;
+  int hi = 32 - __clz(mn ^ mx);  // bits [hi-1, 0] still differ
+  uint32_t mask = hi == 32 ? 0u : ~((1u << hi) - 1u);
+  uint32_t prefix = mn & mask;
+  int remaining = kth;
+  while (hi > 0) {
+    const int w = min(8, hi), shift = hi - w;
+    const uint32_t nb = 1u << w;
+    for (uint32_t i = lane; i < 256; i += 32) hist[i] = 0;
     __syncwarp();
-    uint32_t local[8], s = 0;
+#pragma unroll
+    for (int j = 0; j < NPL; ++j)
+      if (j * 32 + lane < n && (key[j] & mask) == prefix) atomicAdd(&hist[(key[j] >> shift) & (nb - 1)], 1u);
+    __syncwarp();
+    uint32_t local[8], sum = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
       local[j] = hist[lane * 8 + j];
-      s += local[j];
+      sum += local[j];
     }
-    uint32_t inc = s;
+    uint32_t inc = sum;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
       const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
       if (lane >= o) inc += v;
     }
-    const uint32_t excl = inc - s;
+    const uint32_t excl = inc - sum;
     const uint32_t hit = __ballot_sync(0xffffffffu, excl < (uint32_t)remaining && inc >= (uint32_t)remaining);
     const int owner = __ffs(hit) - 1;
     uint32_t bin = 0, before = 0;
     if (lane == owner) {
       uint32_t c = excl;
-      for (int j = 0; j < 8; ++j) {
+#pragma unroll
+      for (int j = 0; j < 8; ++j)
         if (c + local[j] >= (uint32_t)remaining) {
           bin = lane * 8 + j;
           before = c;
           break;
+        } else {
+          c += local[j];
         }
-        c += local[j];
-      }
     }
     bin = __shfl_sync(0xffffffffu, bin, owner);
     before = __shfl_sync(0xffffffffu, before, owner);
     remaining -= (int)before;
     prefix |= bin << shift;
-    mask |= 255u << shift;
+    mask |= (nb - 1) << shift;
+    hi = shift;
     __syncwarp();
   }
-  return sortable_f32(prefix);
+  return prefix;
 }
 
-// Bound and trim list L to its k' smallest screening distances (ties kept).
-template <class F>
+// Bound and trim list L to its k' smallest screening distances (ties kept):
+// the list (n <= 32 * NPL entries) is read once into registers, its k'-th
+// key selected there, the bound shared through T_global, and the kept
+// entries written back in order.
+template <class F, int NPL>
 __device__ __noinline__ void bcompact(Candidate *list, BScreenSmem<F> &sm, int L, int wslot, uint32_t kprime,
                                       uint32_t capb, uint32_t *T_global, uint32_t *ovf) {
   const int lane = threadIdx.x & 31;
   const int n = sm.cnt[L];
   const int32_t qi = sm.lq[L];
   float T = sm.thr[L];
-  if (n >= (int)kprime) T = fminf(T, warp_select_kth(list, n, (int)kprime, sm.hist[wslot]));
+  uint32_t key[NPL], pos[NPL];
+  const uint2 *src = reinterpret_cast<const uint2 *>(list);
+#pragma unroll
+  for (int j = 0; j < NPL; ++j) {
+    const int i = j * 32 + lane;
+    uint2 c = make_uint2(0xffffffffu, 0u);
+    if (i < n) c = src[i];
+    key[j] = i < n ? f32_sortable(__uint_as_float(c.x)) : 0xffffffffu;
+    pos[j] = c.y;
+  }
+  if (n >= (int)kprime) T = fminf(T, sortable_f32(warp_kth_regs<NPL>(key, n, (int)kprime, sm.hist[wslot])));
   const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
   if (Tg < T) T = Tg;
   if (lane == 0 && T < Tg) atomicMin(T_global + qi, f32_sortable(T));
-  // in-place stable compaction of the entries with ds <= T
+  const uint32_t tk = f32_sortable(T);
   int kept = 0;
   const uint32_t lt = (1u << lane) - 1u;
-  for (int base = 0; base < n; base += 32) {
-    const int i = base + lane;
-    Candidate c;
-    bool keep = false;
-    if (i < n) {
-      c = list[i];
-      keep = c.ds <= T;
-    }
+  uint2 *dst = reinterpret_cast<uint2 *>(list);
+  __syncwarp();
+#pragma unroll
+  for (int j = 0; j < NPL; ++j) {
+    const bool keep = j * 32 + lane < n && key[j] <= tk;
     const uint32_t b = __ballot_sync(0xffffffffu, keep);
-    __syncwarp();
-    if (keep) list[kept + __popc(b & lt)] = c;
+    if (keep) dst[kept + __popc(b & lt)] = make_uint2(__float_as_uint(sortable_f32(key[j])), pos[j]);
     kept += __popc(b);
-    __syncwarp();
   }
+  __syncwarp();
   if (lane == 0) {
     if (kept > (int)capb - BR) {
       ovf[qi] = 1u;  // a tie flood: the exact scan answers this query
@@ -394,7 +420,7 @@ __device__ __noinline__ void bcompact(Candidate *list, BScreenSmem<F> &sm, int L
   __syncwarp();
 }
 
-template <class F>
+template <class F, int NPL>
 __global__ void __launch_bounds__(B_THREADS, 2)
     k_screen_tc(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles,
                   const unsigned char *__restrict__ atiles, const int32_t *__restrict__ lane_q,
@@ -553,7 +579,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
         const int b = __ffs(msk) - 1;
         msk &= msk - 1;
         const int Lb = wg * 32 + b;
-        bcompact(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+        bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
       }
       cnt = sm.cnt[L];
       T = sm.thr[L];
@@ -567,7 +593,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       for (int b = 0; b < 32; ++b) {
         const int Lb = wg * 32 + b;
         if (sm.cnt[Lb] > 0 && sm.lq[Lb] >= 0)
-          bcompact(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+          bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
       }
       out_cnt[(uint64_t)item_id * BQ + L] = (uint32_t)sm.cnt[L];
     }
@@ -847,13 +873,16 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
       k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), d_desc, (__nv_bfloat16 *)d_at,
                                                d_lqs);
     // per device context, so set on every call (cheap)
-    FKNN_CUDA(cudaFuncSetAttribute(k_screen_tc<F>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    // the compaction holds a whole list in registers: 32 x NPL >= capb
+    auto screen = capb <= 512 ? k_screen_tc<F, 16> : capb <= 768 ? k_screen_tc<F, 24>
+                : capb <= 1024 ? k_screen_tc<F, 32> : k_screen_tc<F, 40>;
+    FKNN_CUDA(cudaFuncSetAttribute(screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)sizeof(BScreenSmem<F>)));
     FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)sizeof(RerankSmem)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
     void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
-    k_screen_tc<F><<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
+    screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
         (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_lqs,
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
