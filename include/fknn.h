@@ -59,6 +59,17 @@ typedef struct fknn_index_opts {
   uint64_t hbm_budget;  /* bytes the index may hold on the device; 0 = no limit */
 } fknn_index_opts;
 
+/* Plan and kernel parameters of one search mode, per index (the autotuner
+ * in fknn/autotune.py picks them per device, base size and mode). */
+typedef struct fknn_tuning {
+  uint32_t list_slack;       /* BF16/FP8: candidate-list room beyond k' between trims, rows (>= 256) */
+  uint32_t items_per_sm;     /* contraction work items per SM: load balance against candidate traffic */
+  uint32_t min_chunk_blocks; /* shortest row chunk of a work item, in row blocks (64 rows exact, 128 BF16/FP8) */
+  uint32_t bound_refresh;    /* BF16/FP8: sub-tiles between reloads of the shared per-query bound (0 = at trims) */
+  uint32_t pilot_stride;     /* BF16/FP8: a pilot pass over every pilot_stride-th row block first seeds the
+                                bound of long queries (0 or 1 = no pilot) */
+} fknn_tuning;
+
 typedef struct fknn_search_opts {
   int mode;             /* FKNN_MODE_* */
   uint32_t kprime;      /* candidate width for the reduced-precision modes (0 = default 400) */
@@ -110,6 +121,14 @@ int fknn_index_bytes(const fknn_index *index, uint64_t *bytes);
  * Returns when the results are in ids/dists (host or device). */
 int fknn_search(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,
                 int mode, uint32_t *ids, float *dists, void *stream);
+
+/* Sets / reads the tuning of one search mode (FKNN_MODE_*) of an index.
+ * Zero list_slack / items_per_sm / min_chunk_blocks keep their current
+ * value; bound_refresh and pilot_stride are always taken.  Exact-mode results do not depend
+ * on the tuning; reduced-precision results depend on it only through which
+ * equal-screening-distance candidates are kept. */
+int fknn_index_set_tuning(fknn_index *index, int mode, const fknn_tuning *t);
+int fknn_index_get_tuning(const fknn_index *index, int mode, fknn_tuning *t);
 
 /* As fknn_search with options and statistics (stats may be NULL). */
 int fknn_search_ex(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,

@@ -428,7 +428,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
                   const float2 *__restrict__ lane_qs, const unsigned char *__restrict__ blocks_t,
                   const unsigned char *__restrict__ blocks_c, uint32_t *__restrict__ T_global,
                   uint32_t *__restrict__ ovf, Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt,
-                  uint32_t kprime, uint32_t capb, int *err) {
+                  uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride, int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   BScreenSmem<F> &sm = *reinterpret_cast<BScreenSmem<F> *>(smem_raw);
   constexpr uint32_t TB = Tiles<F>::BYTES;
@@ -437,7 +437,8 @@ __global__ void __launch_bounds__(B_THREADS, 2)
   const WorkItem it = items[item_id];
   const Tile tl = tiles[it.tile];
   const unsigned char *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
-  const uint32_t nsub = it.blk1 - it.blk0;
+  // every stride-th row block of the item (stride 1: all of them)
+  const uint32_t nsub = (it.blk1 - it.blk0 + stride - 1) / stride;
 
   if (tid == 0) {
     for (int s = 0; s < BS; ++s) {
@@ -471,7 +472,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
         const int st = sub % BS;
         if (sub >= BS && !mbar_wait_bounded(&sm.empty[st], ((sub / BS) - 1) & 1, err)) break;
         mbar_arrive_expect_tx(&sm.full[st], TB);
-        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub) * TB, TB, &sm.full[st]);
+        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub * stride) * TB, TB, &sm.full[st]);
         ++issued;
       }
       mbar_wait_bounded(&sm.abar, 0, err);
@@ -535,7 +536,7 @@ __global__ void __launch_bounds__(B_THREADS, 2)
         break;
       }
       tc_fence_after();
-      const uint32_t p0 = (it.blk0 + sub) * BR;
+      const uint32_t p0 = (it.blk0 + sub * stride) * BR;
       const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
       const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
       // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc)
@@ -556,13 +557,24 @@ __global__ void __launch_bounds__(B_THREADS, 2)
             if (c + j >= r0 && c + j < r1) m = fmaxf(m, v[j]);
         }
         if (m >= cq) {
+          // pushes in groups of 8 columns: a group runs only if one of the
+          // warp's queries has a candidate in it
 #pragma unroll
-          for (int j = 0; j < 32; ++j) {
-            if (v[j] >= cq && c + j >= r0 && c + j < r1) {
-              Candidate cd;
-              cd.ds = fmaf(-2.f * sc, v[j], qn);
-              cd.pos = p0 + c + j;
-              list[cnt++] = cd;
+          for (int g = 0; g < 32; g += 8) {
+            float mg = -INFINITY;
+#pragma unroll
+            for (int j = g; j < g + 8; ++j)
+              if (c + j >= r0 && c + j < r1) mg = fmaxf(mg, v[j]);
+            if (mg >= cq) {
+#pragma unroll
+              for (int j = g; j < g + 8; ++j) {
+                if (v[j] >= cq && c + j >= r0 && c + j < r1) {
+                  Candidate cd;
+                  cd.ds = fmaf(-2.f * sc, v[j], qn);
+                  cd.pos = p0 + c + j;
+                  list[cnt++] = cd;
+                }
+              }
             }
           }
         }
@@ -580,6 +592,11 @@ __global__ void __launch_bounds__(B_THREADS, 2)
         msk &= msk - 1;
         const int Lb = wg * 32 + b;
         bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+      }
+      // other items of the same query tighten the shared bound meanwhile
+      if (refresh && sub % refresh == refresh - 1 && qi >= 0) {
+        const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+        if (Tg < sm.thr[L]) sm.thr[L] = Tg;
       }
       cnt = sm.cnt[L];
       T = sm.thr[L];
@@ -629,8 +646,8 @@ __global__ void __launch_bounds__(RR_THREADS)
                    const float *__restrict__ q, const float *__restrict__ vecs, const uint32_t *__restrict__ perm_t,
                    const uint32_t *__restrict__ perm_c, const uint32_t *__restrict__ ovf,
                    uint32_t *__restrict__ ovf_list, uint32_t *__restrict__ ovf_count, uint32_t k, uint32_t kprime,
-                   uint32_t capb, uint32_t *__restrict__ ids, float *__restrict__ dists,
-                   uint32_t *__restrict__ n_f64) {
+                   uint32_t capb, const uint32_t *__restrict__ seeded, uint32_t *__restrict__ ids,
+                   float *__restrict__ dists, uint32_t *__restrict__ n_f64) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   RerankSmem &sm = *reinterpret_cast<RerankSmem *>(smem_raw);
   const int tid = threadIdx.x;
@@ -657,7 +674,9 @@ __global__ void __launch_bounds__(RR_THREADS)
   }
   __syncthreads();
   const int M = sm.total;
-  if (M > RR_CAP) {
+  // a pilot bound that kept fewer than k' rows was set too low: the exact
+  // scan answers the query
+  if (M > RR_CAP || (seeded && seeded[qi] && M < (int)kprime)) {
     if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
     return;
   }
@@ -746,6 +765,22 @@ __global__ void __launch_bounds__(RR_THREADS)
   }
 }
 
+// Seeds the shared bound of every long query from the pilot pass: T_A is
+// the r-th smallest screening distance over every stride-th row block, an
+// estimate of the k'-th over all rows (r is chosen so that it lies above it
+// with high probability; the merge catches the rest).
+__global__ void k_seed_bounds(const uint32_t *__restrict__ big_q, uint32_t nbig, const QueryDesc *__restrict__ desc,
+                              const uint32_t *__restrict__ T_A, const uint32_t *__restrict__ ovf_A,
+                              uint32_t min_rows, uint32_t *__restrict__ T_global, uint32_t *__restrict__ seeded) {
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x) {
+    const uint32_t qi = big_q[i];
+    const uint32_t inf = f32_sortable(INFINITY);
+    const bool s = desc[qi].e - desc[qi].s >= min_rows && T_A[qi] < inf && !ovf_A[qi];
+    T_global[qi] = s ? T_A[qi] : inf;
+    seeded[qi] = s ? 1u : 0u;
+  }
+}
+
 inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 }  // namespace
@@ -793,10 +828,13 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   QueryDesc *d_desc, *h_desc;
   float *h_meta;
   if ((rc = prepare_queries(idx, d_q, d_meta, nq, st, &d_desc, &h_desc, &h_meta))) return rc;
-  // candidate slots per (item, query): k' plus one sub-tile of pushes plus slack
-  const uint32_t capb = (uint32_t)align_up(kprime + 2 * BR, 128);
+  const fknn_tuning tune = idx->tuning[F::kFP8 ? FKNN_MODE_FP8_RERANK : FKNN_MODE_BF16_RERANK];
+  // candidate slots per (item, query): k' plus the pushes between trims; a
+  // list holds at most 1280 (32 lanes x 40 registers in the trim)
+  const uint32_t capb =
+      (uint32_t)std::min<size_t>(1280, align_up(kprime + std::max<uint32_t>(tune.list_slack, 2 * BR), 128));
   auto t0 = std::chrono::steady_clock::now();
-  Plan P;
+  Plan &P = idx->plan;
   PlanShape shape;
   shape.tq = BQ;
   shape.blk_rows = BR;
@@ -806,15 +844,17 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   const uint64_t tiles_est = std::max<uint64_t>(1, (nq + BQ - 1) / BQ);
   shape.max_items_per_tile = (uint32_t)std::max<uint64_t>(
       1, std::min<uint64_t>(RR_CAP / capb, (8ull << 30) / (per_item * tiles_est)));
-  shape.min_chunk_blocks = 8;
-  shape.target_items = 148 * 2 * 3;
+  shape.min_chunk_blocks = tune.min_chunk_blocks;
+  shape.target_items = idx->num_sms * tune.items_per_sm;
   make_plan(h_desc, h_meta, nq, n, shape, P);
   auto t1 = std::chrono::steady_clock::now();
   const uint32_t ntile = (uint32_t)P.tiles.size(), nitems = (uint32_t)P.items.size();
   const uint32_t nbig = (uint32_t)P.big.size(), nsmall = (uint32_t)P.small.size();
-  std::vector<uint32_t> slot(nitems);
+  std::vector<uint32_t> &slot = P.w_slot;
+  slot.resize(nitems);
   {
-    std::vector<uint32_t> fill(ntile);
+    std::vector<uint32_t> &fill = P.w_fill;
+    fill.resize(ntile);
     for (uint32_t t = 0; t < ntile; ++t) fill[t] = P.tiles[t].item0;
     for (uint32_t s = 0; s < nitems; ++s) slot[fill[P.items[s].tile]++] = s;
   }
@@ -853,6 +893,13 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   if ((rc = launch_fill_u32(T_global, nq, f32_sortable(INFINITY), st))) return rc;
   FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
   FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 8, st));
+  // pilot state: bound estimate, seeded flag, pilot overflow per query
+  uint32_t *d_pilot = nullptr, *seeded = nullptr;
+  if (tune.pilot_stride > 1) {
+    if ((rc = ws_get(idx, 11, (size_t)nq * 12, (void **)&d_pilot))) return rc;
+    seeded = d_pilot + nq;
+    FKNN_CUDA(cudaMemsetAsync(seeded, 0, (size_t)nq * 4, st));
+  }
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   if (stats)
     for (auto &e : ev) FKNN_CUDA(cudaEventCreate(&e));
@@ -882,16 +929,36 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
                                    (int)sizeof(RerankSmem)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
     void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
+    const uint32_t stride = tune.pilot_stride;
+    if (stride > 1) {
+      // pilot: every stride-th row block with a short list; its r-th
+      // distance seeds the bound of queries with long slabs
+      // the k'-th of all rows ranks about k'/stride in the sample; r = 3 k'/stride
+      // + 8 lies above it but for a vanishing fraction of queries
+      const uint32_t r = std::min<uint32_t>(kprime, (3 * kprime + stride - 1) / stride + 8);
+      uint32_t *T_A = d_pilot, *ovf_A = d_pilot + 2 * (size_t)nq;
+      if ((rc = launch_fill_u32(T_A, nq, f32_sortable(INFINITY), st))) return rc;
+      FKNN_CUDA(cudaMemsetAsync(ovf_A, 0, (size_t)nq * 4, st));
+      screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
+          (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at,
+          (const int32_t *)(d_blob + o_lq), (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le),
+          d_lqs, (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A,
+          d_out, d_ocnt, r, capb, 0, stride, idx->d_flag);
+      k_seed_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>((nbig + 255) / 256, 1184)), 256, 0, st>>>(
+          (const uint32_t *)(d_blob + o_big), nbig, d_desc, T_A, ovf_A, 16 * stride * BR, T_global, seeded);
+      g_launches += 3;
+    }
     screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
         (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_lqs,
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
-        d_ocnt, kprime, capb, idx->d_flag);
+        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->d_flag);
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     k_merge_rerank<<<nbig, RR_THREADS, sizeof(RerankSmem), st>>>(
         (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
         (const Tile *)(d_blob + o_tiles), (const uint32_t *)(d_blob + o_slot), d_out, d_ocnt, d_desc, d_q, idx->vecs,
-        OT.perm, OC.perm, ovf, ovf_list, ovf_count, k, kprime, capb, d_ids, d_dists, n_f64);
+        OT.perm, OC.perm, ovf, ovf_list, ovf_count, k, kprime, capb, stride > 1 ? seeded : nullptr, d_ids, d_dists,
+        n_f64);
     g_launches += 3;
   }
   if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));

@@ -137,6 +137,8 @@ int make_index_view(fknn_index *base, fknn_index **out) {
     v->fp8_blocks[o] = base->fp8_blocks[o];
   }
   v->fp8_scale = base->fp8_scale;
+  for (int m = 0; m < 3; ++m) v->tuning[m] = base->tuning[m];
+  v->num_sms = base->num_sms;
   v->is_view = true;
   cudaError_t e = cudaSetDevice(v->device);
   if (e == cudaSuccess) e = cudaMalloc(&v->d_flag, 64);
@@ -218,6 +220,9 @@ int fknn_index_create(const float *vecs, const float *labels, const float *ts, u
   e = cudaSetDevice(idx->device);
   if (e != cudaSuccess) rc = cuda_fail(e, "cudaSetDevice");
   if (!rc) {
+    int sms = 0;
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, idx->device) == cudaSuccess && sms > 0)
+      idx->num_sms = sms;
     e = cudaStreamCreateWithFlags(&idx->own_stream, cudaStreamNonBlocking);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaStreamCreate");
   }
@@ -339,6 +344,36 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     set_error("fknn_search: a bounded device wait gave up; affected queries were answered by the exact scan");
   }
   if (stats) stats->kernel_launches = g_launches;
+  return FKNN_OK;
+}
+
+int fknn_index_set_tuning(fknn_index *index, int mode, const fknn_tuning *t) {
+  if (!index || !t || mode < 0 || mode > 2) {
+    set_error("fknn_index_set_tuning: NULL argument or unknown mode");
+    return FKNN_EINVAL;
+  }
+  if ((t->list_slack && (t->list_slack < 256 || t->list_slack > 1024)) || t->items_per_sm > 64 ||
+      t->min_chunk_blocks > 4096 || t->bound_refresh > 4096 || t->pilot_stride > 1024) {
+    set_error("fknn_index_set_tuning: list_slack in [256, 1024], items_per_sm <= 64, min_chunk_blocks <= 4096, "
+              "bound_refresh <= 4096, pilot_stride <= 1024");
+    return FKNN_EINVAL;
+  }
+  std::lock_guard<std::mutex> lock(index->mu);
+  fknn_tuning &d = index->tuning[mode];
+  if (t->list_slack) d.list_slack = t->list_slack;
+  if (t->items_per_sm) d.items_per_sm = t->items_per_sm;
+  if (t->min_chunk_blocks) d.min_chunk_blocks = t->min_chunk_blocks;
+  d.bound_refresh = t->bound_refresh;
+  d.pilot_stride = t->pilot_stride;
+  return FKNN_OK;
+}
+
+int fknn_index_get_tuning(const fknn_index *index, int mode, fknn_tuning *t) {
+  if (!index || !t || mode < 0 || mode > 2) {
+    set_error("fknn_index_get_tuning: NULL argument or unknown mode");
+    return FKNN_EINVAL;
+  }
+  *t = index->tuning[mode];
   return FKNN_OK;
 }
 

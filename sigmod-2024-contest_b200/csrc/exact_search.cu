@@ -760,11 +760,61 @@ int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *cou
 // Groups queries into 64-query tiles whose slabs overlap (same order and
 // predicate class, start bucket, then end), and cuts each tile's union
 // range into row chunks.
+namespace {
+
+// Sorts plan keys by (order, cls, bucket, e, s, qi): an LSD radix sort on
+// the packed 128-bit image (order 1 bit, cls 2, bucket 29, e 32 | s 32, qi
+// 32), 16-bit digits, passes whose digit is constant skipped.
+void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
+  const size_t m = keys.size();
+  if (m < 2) return;
+  auto &hi = W.w_hi, &lo = W.w_lo, &hi2 = W.w_hi2, &lo2 = W.w_lo2;
+  auto &ix = W.w_ix, &ix2 = W.w_ix2, &cnt = W.w_cnt;
+  hi.resize(m);
+  lo.resize(m);
+  hi2.resize(m);
+  lo2.resize(m);
+  ix.resize(m);
+  ix2.resize(m);
+  cnt.resize(65537);
+  for (size_t i = 0; i < m; ++i) {
+    const PlanKey &k = keys[i];
+    hi[i] = ((uint64_t)k.order << 63) | ((uint64_t)(k.cls & 3) << 61) | ((k.bucket & 0x1fffffffull) << 32) | k.e;
+    lo[i] = ((uint64_t)k.s << 32) | k.qi;
+    ix[i] = (uint32_t)i;
+  }
+  for (int pass = 0; pass < 8; ++pass) {
+    const bool upper = pass >= 4;
+    const int shift = (pass & 3) * 16;
+    const std::vector<uint64_t> &src = upper ? hi : lo;
+    std::fill(cnt.begin(), cnt.end(), 0u);
+    for (size_t i = 0; i < m; ++i) ++cnt[((src[i] >> shift) & 0xffff) + 1];
+    if (cnt[((src[0] >> shift) & 0xffff) + 1] == m) continue;  // one digit value: order unchanged
+    for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
+    for (size_t i = 0; i < m; ++i) {
+      const uint32_t pos = cnt[(src[i] >> shift) & 0xffff]++;
+      hi2[pos] = hi[i];
+      lo2[pos] = lo[i];
+      ix2[pos] = ix[i];
+    }
+    hi.swap(hi2);
+    lo.swap(lo2);
+    ix.swap(ix2);
+  }
+  auto &out = W.w_keys2;
+  out.resize(m);
+  for (size_t i = 0; i < m; ++i) out[i] = keys[ix[i]];
+  keys.swap(out);
+}
+
+}  // namespace
+
 void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, const PlanShape &shape,
                Plan &P) {
   const int TQ = shape.tq, BLK = shape.blk_rows;
-  std::vector<uint32_t> big;
-  big.reserve(nq);
+  P.reset();
+  std::vector<uint32_t> &big = P.w_big;
+  big.clear();
   for (uint32_t i = 0; i < nq; ++i) {
     const uint32_t len = desc[i].e - desc[i].s;
     P.pairs_passing += len;
@@ -779,12 +829,9 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
   // start buckets: about sqrt(#queries/64) per class so a tile spans little
   const uint64_t nb_all = std::max<uint64_t>(1, (uint64_t)std::sqrt((double)big.size() / 64.0));
   const uint64_t bw = std::max<uint64_t>(BLK, (n + nb_all - 1) / nb_all);
-  struct Key {
-    uint32_t order, cls;
-    uint64_t bucket;
-    uint32_t s, e, qi;
-  };
-  std::vector<Key> keys(big.size());
+  using Key = PlanKey;
+  std::vector<Key> &keys = P.w_keys;
+  keys.resize(big.size());
   for (size_t j = 0; j < big.size(); ++j) {
     const uint32_t i = big[j];
     const QueryDesc &d = desc[i];
@@ -797,19 +844,11 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
     kk.qi = i;
     keys[j] = kk;
   }
-  std::sort(keys.begin(), keys.end(), [](const Key &a, const Key &b) {
-    if (a.order != b.order) return a.order < b.order;
-    if (a.cls != b.cls) return a.cls < b.cls;
-    if (a.bucket != b.bucket) return a.bucket < b.bucket;
-    if (a.e != b.e) return a.e < b.e;
-    if (a.s != b.s) return a.s < b.s;
-    return a.qi < b.qi;
-  });
+  sort_keys(keys, P);
   // greedy tiles
-  struct TileTmp {
-    uint32_t first, count, S, E, order;
-  };
-  std::vector<TileTmp> tt;
+  using TileTmp = PlanTile;
+  std::vector<TileTmp> &tt = P.w_tiles;
+  tt.clear();
   size_t i = 0;
   while (i < keys.size()) {
     TileTmp t{(uint32_t)i, 1, keys[i].s, keys[i].e, keys[i].order};
@@ -846,7 +885,8 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
   P.big.reserve(big.size());
   P.big_tile.reserve(big.size());
   P.big_lane.reserve(big.size());
-  std::vector<WorkItem> items;
+  std::vector<WorkItem> &items = P.w_items;
+  items.clear();
   for (size_t t = 0; t < ntile; ++t) {
     const TileTmp &T = tt[t];
     for (uint32_t l = 0; l < T.count; ++l) {
@@ -882,14 +922,15 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
     if (P.tiles[a.tile].order != P.tiles[b.tile].order) return P.tiles[a.tile].order < P.tiles[b.tile].order;
     return a.blk0 < b.blk0;
   });
-  std::vector<uint32_t> per_tile(ntile + 1, 0);
+  std::vector<uint32_t> &per_tile = P.w_per_tile;
+  per_tile.assign(ntile + 1, 0);
   for (auto &w : items) per_tile[w.tile + 1]++;
   for (size_t t = 0; t < ntile; ++t) per_tile[t + 1] += per_tile[t];
   for (size_t t = 0; t < ntile; ++t) {
     P.tiles[t].item0 = per_tile[t];
     P.tiles[t].item1 = per_tile[t + 1];
   }
-  P.items = std::move(items);
+  P.items.swap(items);
 }
 
 int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,
@@ -947,14 +988,14 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
 
   // 2. plan
   auto t0 = std::chrono::steady_clock::now();
-  Plan P;
+  Plan &P = idx->plan;
   PlanShape shape;
   shape.tq = TQ;
   shape.blk_rows = BLK;
   shape.small_slab = SMALL_SLAB;
   shape.max_items_per_tile = MAX_ITEMS_PER_TILE;
-  shape.min_chunk_blocks = 16;
-  shape.target_items = 148 * 2 * 8;
+  shape.min_chunk_blocks = idx->tuning[FKNN_MODE_EXACT_FP32].min_chunk_blocks;
+  shape.target_items = idx->num_sms * idx->tuning[FKNN_MODE_EXACT_FP32].items_per_sm;
   make_plan(h_desc, h_meta, nq, n, shape, P);
   auto t1 = std::chrono::steady_clock::now();
   const uint32_t ntile = (uint32_t)P.tiles.size(), nitems = (uint32_t)P.items.size();
@@ -962,9 +1003,11 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
 
   // item slots: the merge reads a tile's lists through tile.item0..item1 of
   // a slot table, the screen writes each item's lists at its launch slot.
-  std::vector<uint32_t> slot_of_tile_item(nitems);
+  std::vector<uint32_t> &slot_of_tile_item = P.w_slot;
+  slot_of_tile_item.resize(nitems);
   {
-    std::vector<uint32_t> fill(ntile);
+    std::vector<uint32_t> &fill = P.w_fill;
+    fill.resize(ntile);
     for (uint32_t t = 0; t < ntile; ++t) fill[t] = P.tiles[t].item0;
     for (uint32_t s = 0; s < nitems; ++s) slot_of_tile_item[fill[P.items[s].tile]++] = s;
   }

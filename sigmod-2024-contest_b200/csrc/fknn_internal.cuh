@@ -107,6 +107,21 @@ struct Candidate {
 
 // Host plan of one search call: which queries take the row-by-row exact
 // scan, and the query tiles / row-chunk work items of the contraction.
+// Sort key of a query in the plan: (order, cls, bucket, e, s, qi).
+struct PlanKey {
+  uint32_t order, cls;
+  uint64_t bucket;
+  uint32_t s, e, qi;
+};
+
+struct PlanTile {
+  uint32_t first, count, S, E, order;
+};
+
+// A search plan.  It lives in its index (or view) and is rebuilt by every
+// call; the vectors keep their capacity between calls, so planning touches
+// no fresh pages (first-touch faults of multi-MB vectors cost more than the
+// planning itself).
 struct Plan {
   std::vector<uint32_t> small;                 // query ids for the exact scan
   std::vector<uint32_t> big, big_tile, big_lane;
@@ -115,6 +130,24 @@ struct Plan {
   std::vector<int32_t> lane_q;
   std::vector<uint32_t> lane_s, lane_e;
   uint64_t pairs_screened = 0, pairs_passing = 0, pairs_contraction = 0;
+  // working storage
+  std::vector<uint32_t> w_big, w_ix, w_ix2, w_cnt, w_per_tile, w_slot, w_fill;
+  std::vector<uint64_t> w_hi, w_lo, w_hi2, w_lo2;
+  std::vector<PlanKey> w_keys, w_keys2;
+  std::vector<PlanTile> w_tiles;
+  std::vector<WorkItem> w_items;
+  void reset() {
+    small.clear();
+    big.clear();
+    big_tile.clear();
+    big_lane.clear();
+    tiles.clear();
+    items.clear();
+    lane_q.clear();
+    lane_s.clear();
+    lane_e.clear();
+    pairs_screened = pairs_passing = pairs_contraction = 0;
+  }
 };
 
 struct PlanShape {
@@ -171,6 +204,10 @@ struct fknn_index {
   fknn::HostBuf hs[8];
   int *d_flag = nullptr;
   cudaStream_t own_stream = nullptr;
+  fknn::Plan plan;  // rebuilt by every search; capacity kept
+  // per-mode plan / kernel parameters (fknn_index_set_tuning) and the SM count
+  fknn_tuning tuning[3] = {{0, 16, 16, 0, 0}, {256, 6, 8, 0, 16}, {256, 6, 8, 0, 16}};
+  int num_sms = 148;
   // a view shares the device data of another index and owns only its
   // per-call scratch (ws, hs, d_flag), so views search concurrently
   bool is_view = false;

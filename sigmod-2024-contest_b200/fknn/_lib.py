@@ -54,6 +54,14 @@ class IndexOpts(Structure):
     _fields_ = [("device", c_int), ("build_bf16", c_int), ("build_fp8", c_int), ("hbm_budget", c_uint64)]
 
 
+class Tuning(Structure):
+    _fields_ = [("list_slack", c_uint32), ("items_per_sm", c_uint32), ("min_chunk_blocks", c_uint32),
+                ("bound_refresh", c_uint32), ("pilot_stride", c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 class SearchOpts(Structure):
     _fields_ = [("mode", c_int), ("kprime", c_uint32)]
 
@@ -116,6 +124,8 @@ SIGNATURES = {
                                   POINTER(c_void_p)]),
     "fknn_index_destroy": (c_int, [c_void_p]),
     "fknn_index_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
+    "fknn_index_set_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),
+    "fknn_index_get_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),
     "fknn_search": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p, c_void_p, c_void_p]),
     "fknn_search_ex": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, POINTER(SearchOpts), c_void_p,
                                c_void_p, c_void_p, POINTER(SearchStats)]),

@@ -25,7 +25,7 @@ import numpy as np
 
 from . import _lib
 from ._lib import (MODE_BF16_RERANK, MODE_EXACT_FP32, MODE_FP8_RERANK, IndexOpts, SearchOpts, SearchStats,
-                   ServerOpts, ServerStats, check, load)
+                   ServerOpts, ServerStats, Tuning, check, load)
 
 DIM = 100
 K = 100  # utils.h:88
@@ -139,6 +139,20 @@ class Index:
         if return_stats:
             return ids, dists, st.as_dict()
         return ids, dists
+
+    def set_tuning(self, mode: int, list_slack: int = 0, items_per_sm: int = 0, min_chunk_blocks: int = 0,
+                   bound_refresh: int = 0, pilot_stride: int = None) -> None:
+        """fknn_index_set_tuning: plan / kernel parameters of one mode
+        (pilot_stride None keeps the current one)."""
+        if pilot_stride is None:
+            pilot_stride = self.get_tuning(mode)["pilot_stride"]
+        check(load().fknn_index_set_tuning(self._h, mode, byref(Tuning(list_slack, items_per_sm, min_chunk_blocks,
+                                                                        bound_refresh, pilot_stride))))
+
+    def get_tuning(self, mode: int) -> dict:
+        t = Tuning()
+        check(load().fknn_index_get_tuning(self._h, mode, byref(t)))
+        return t.as_dict()
 
     def count_matches(self, metas) -> np.ndarray:
         metas = np.ascontiguousarray(metas, dtype=np.float32)
