@@ -33,6 +33,7 @@ constexpr int BS = 2;                         // shared-memory stages for row bl
 constexpr int B_EPI_WARPS = 4;
 constexpr int B_THREADS = (2 + B_EPI_WARPS) * 32;  // producer, MMA issuer, 4 epilogue warps
 constexpr uint32_t TMEM_COLS = 2 * BR;        // double-buffered accumulator
+constexpr int STAGE_ROW = 36;                 // floats per lane row of the push staging area
 
 // Operand formats of the tensor-core screen.  Both operands are K-major,
 // no swizzle, in core matrices of 8 rows x 16 bytes; every MMA consumes 32
@@ -296,9 +297,16 @@ struct BScreenSmem {
   int cnt[BQ];
   int32_t lq[BQ];
   uint32_t hist[B_EPI_WARPS][256];
+  // per epilogue lane, the 32 accumulator columns of a chunk that has
+  // candidates (rows padded to 36 floats: conflict-free 16-byte stores)
+  float stage[B_EPI_WARPS][32 * STAGE_ROW];
   uint64_t full[BS], empty[BS], accfull[2], accempty[2], abar;
   uint32_t tmem_base;
 };
+
+// two screening CTAs share an SM (228 KB of shared memory, 1 KB reserved per CTA)
+static_assert(sizeof(BScreenSmem<FmtBF16>) <= 113 * 1024 && sizeof(BScreenSmem<FmtFP8>) <= 113 * 1024,
+              "screen shared memory must leave room for two CTAs per SM");
 
 // kth smallest (1-based) of the n keys held NPL per lane (element
 // j*32 + lane in key[j]; keys past n ignored): a warp radix select that
@@ -557,25 +565,28 @@ __global__ void __launch_bounds__(B_THREADS, 2)
             if (c + j >= r0 && c + j < r1) m = fmaxf(m, v[j]);
         }
         if (m >= cq) {
-          // pushes in groups of 8 columns: a group runs only if one of the
-          // warp's queries has a candidate in it
+          // this lane's candidates as a bit mask; their values are read back
+          // from shared memory, so the push loop runs once per candidate of
+          // the lane with the most, not once per column
+          uint32_t mask = 0;
+          if (whole) {
 #pragma unroll
-          for (int g = 0; g < 32; g += 8) {
-            float mg = -INFINITY;
+            for (int j = 0; j < 32; ++j) mask |= (v[j] >= cq ? 1u : 0u) << j;
+          } else {
 #pragma unroll
-            for (int j = g; j < g + 8; ++j)
-              if (c + j >= r0 && c + j < r1) mg = fmaxf(mg, v[j]);
-            if (mg >= cq) {
+            for (int j = 0; j < 32; ++j) mask |= (v[j] >= cq && c + j >= r0 && c + j < r1 ? 1u : 0u) << j;
+          }
+          float *row = &sm.stage[wslot][lane * STAGE_ROW];
 #pragma unroll
-              for (int j = g; j < g + 8; ++j) {
-                if (v[j] >= cq && c + j >= r0 && c + j < r1) {
-                  Candidate cd;
-                  cd.ds = fmaf(-2.f * sc, v[j], qn);
-                  cd.pos = p0 + c + j;
-                  list[cnt++] = cd;
-                }
-              }
-            }
+          for (int j = 0; j < 32; j += 4)
+            *reinterpret_cast<float4 *>(row + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+          while (mask) {
+            const int j = __ffs(mask) - 1;
+            mask &= mask - 1;
+            Candidate cd;
+            cd.ds = fmaf(-2.f * sc, row[j], qn);
+            cd.pos = p0 + c + j;
+            list[cnt++] = cd;
           }
         }
       }
