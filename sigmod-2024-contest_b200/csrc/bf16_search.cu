@@ -672,16 +672,14 @@ __global__ void __launch_bounds__(RR_THREADS)
   const uint32_t nitems = tl.item1 - tl.item0;
   const QueryDesc dsc = desc[qi];
   for (int d = tid; d < DIM; d += RR_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
-  const uint32_t per = (nitems + RR_THREADS - 1) / RR_THREADS;
-  const uint32_t ib = tid * per, ie = min(ib + per, nitems);
-  uint32_t mine = 0;
-  for (uint32_t i = ib; i < ie; ++i) mine += out_cnt[(uint64_t)item_slot[tl.item0 + i] * BQ + L];
-  sm.cnt_prefix[tid + 1] = mine;
-  if (tid == 0) sm.cnt_prefix[0] = 0;
-  __syncthreads();
+  // candidate counts of the query's items (a tile has at most a few dozen)
   if (tid == 0) {
-    for (int t = 0; t < RR_THREADS; ++t) sm.cnt_prefix[t + 1] += sm.cnt_prefix[t];
-    sm.total = (int)sm.cnt_prefix[RR_THREADS];
+    uint32_t total = nitems > RR_THREADS ? RR_CAP + 1 : 0;  // more items than prefix slots: exact scan
+    for (uint32_t i = 0; i < nitems && i < RR_THREADS; ++i) {
+      sm.cnt_prefix[i] = total;
+      total += out_cnt[(uint64_t)item_slot[tl.item0 + i] * BQ + L];
+    }
+    sm.total = (int)total;
   }
   __syncthreads();
   const int M = sm.total;
@@ -691,18 +689,16 @@ __global__ void __launch_bounds__(RR_THREADS)
     if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
     return;
   }
-  {
-    uint32_t w = sm.cnt_prefix[tid];
-    for (uint32_t i = ib; i < ie; ++i) {
-      const uint64_t item = item_slot[tl.item0 + i];
-      const uint32_t c = out_cnt[item * BQ + L];
-      const Candidate *src = out + (item * BQ + L) * capb;
-      for (uint32_t j = 0; j < c; ++j) {
-        const Candidate cd = src[j];
-        sm.key[w] = cd.ds;
-        sm.val[w] = cd.pos;
-        ++w;
-      }
+  // the whole block copies each item's list
+  for (uint32_t i = 0; i < nitems; ++i) {
+    const uint64_t item = item_slot[tl.item0 + i];
+    const uint32_t base = sm.cnt_prefix[i];
+    const uint32_t c = (i + 1 < nitems ? sm.cnt_prefix[i + 1] : (uint32_t)M) - base;
+    const Candidate *src = out + (item * BQ + L) * capb;
+    for (uint32_t j = tid; j < c; j += RR_THREADS) {
+      const Candidate cd = src[j];
+      sm.key[base + j] = cd.ds;
+      sm.val[base + j] = cd.pos;
     }
   }
   int np2 = 32;

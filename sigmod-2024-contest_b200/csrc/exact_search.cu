@@ -468,17 +468,15 @@ __global__ void __launch_bounds__(MG_THREADS)
   const QueryDesc dsc = desc[qi];
   const float qn = dsc.qn;
   for (int d = tid; d < DIM; d += MG_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
-  // 1. gather the lists (per-thread strip of items, block prefix)
-  const uint32_t per = (nitems + MG_THREADS - 1) / MG_THREADS;
-  const uint32_t ib = tid * per, ie = min(ib + per, nitems);
-  uint32_t mine = 0;
-  for (uint32_t i = ib; i < ie; ++i) mine += out_cnt[(uint64_t)item_slot[tl.item0 + i] * TQ + L];
-  sm.cnt_prefix[tid + 1] = mine;
-  if (tid == 0) sm.cnt_prefix[0] = 0;
-  __syncthreads();
+  // 1. gather the lists: item offsets (a tile has at most a few dozen
+  // items), then the whole block copies each list
   if (tid == 0) {
-    for (int t = 0; t < MG_THREADS; ++t) sm.cnt_prefix[t + 1] += sm.cnt_prefix[t];
-    sm.total = (int)sm.cnt_prefix[MG_THREADS];
+    uint32_t total = nitems > MG_THREADS ? MERGE_CAP + 1 : 0;  // more items than offset slots: exact scan
+    for (uint32_t i = 0; i < nitems && i < MG_THREADS; ++i) {
+      sm.cnt_prefix[i] = total;
+      total += out_cnt[(uint64_t)item_slot[tl.item0 + i] * TQ + L];
+    }
+    sm.total = (int)total;
   }
   __syncthreads();
   const int M = sm.total;
@@ -486,18 +484,15 @@ __global__ void __launch_bounds__(MG_THREADS)
     if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
     return;
   }
-  {
-    uint32_t w = sm.cnt_prefix[tid];
-    for (uint32_t i = ib; i < ie; ++i) {
-      const uint64_t item = item_slot[tl.item0 + i];
-      const uint32_t c = out_cnt[item * TQ + L];
-      const Candidate *src = out + (item * TQ + L) * CAP;
-      for (uint32_t j = 0; j < c; ++j) {
-        Candidate cd = src[j];
-        sm.key[w] = cd.ds;
-        sm.val[w] = cd.pos;
-        ++w;
-      }
+  for (uint32_t i = 0; i < nitems; ++i) {
+    const uint64_t item = item_slot[tl.item0 + i];
+    const uint32_t base = sm.cnt_prefix[i];
+    const uint32_t c = (i + 1 < nitems ? sm.cnt_prefix[i + 1] : (uint32_t)M) - base;
+    const Candidate *src = out + (item * TQ + L) * CAP;
+    for (uint32_t j = tid; j < c; j += MG_THREADS) {
+      const Candidate cd = src[j];
+      sm.key[base + j] = cd.ds;
+      sm.val[base + j] = cd.pos;
     }
   }
   int np2 = 32;
