@@ -52,7 +52,8 @@ def parse():
     ap.add_argument("--nq", type=int, default=None, help="override queries per step")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=1024, help="queries in the CPU-baseline sample")
-    ap.add_argument("--kprime", type=int, default=200, help="candidate width of the BF16 form")
+    ap.add_argument("--kprime", type=int, default=None,
+                    help="candidate width of the BF16 form (default: the autotuned one, else 200)")
     ap.add_argument("--sweep", action="store_true",
                     help="precision sweep instead of the headline: exact, BF16 and FP8 forms at k' in "
                          "--kprimes, recall and distance error against an FP64 oracle sample; one JSON line each")
@@ -64,7 +65,11 @@ def parse():
     ap.add_argument("--rates", default="10000,50000,200000")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-forms", default="bf16,exact")
-    return ap.parse_args()
+    a = ap.parse_args()
+    a.kprime_set = a.kprime is not None
+    if a.kprime is None:
+        a.kprime = 200
+    return a
 
 
 class ClockSampler:
@@ -400,6 +405,11 @@ def main():
     q, metas = datagen.make_queries(nq, w.zipf_s, w.n_labels, w.window, w.balanced_types, 1234 + args.config,
                                     1235 + args.config + 1000 * rank)
     idx = fknn.Index(vecs, labels, ts, device=local, build_bf16=True)
+    # autotuned plan / kernel parameters and k' for this device and base size, if recorded
+    idx.apply_tuning(fknn.MODE_EXACT_FP32)
+    tuned_kp = idx.apply_tuning(fknn.MODE_BF16_RERANK)
+    if tuned_kp and not args.kprime_set:
+        args.kprime = tuned_kp
     stream = torch.cuda.current_stream()
     dq = torch.from_numpy(q).cuda()
     dm = torch.from_numpy(metas).cuda()
@@ -517,6 +527,7 @@ def main():
             "vs_baseline": None, "dtype": "bf16" if use_bf16 else "f32", "data": "synthetic",
             "config": {"workload": w.name, "mode": "bf16_rerank" if use_bf16 else "exact_fp32",
                        "kprime": args.kprime if use_bf16 else None, "n": n, "nq_per_gpu": nq, "k": 100, "d": 100,
+                       "tuning": idx.get_tuning(head_mode),
                        "parallelism": f"replicas{world}" if world > 1 else "single",
                        "l2": "no flush: each step streams the row orders (2 x 404 MB FP32, 2 x 229 MB BF16) > 126 MB L2"},
             "recall_at_100_vs_exact": recall_bf16 if use_bf16 else 1.0,

@@ -149,6 +149,19 @@ class Index:
         check(load().fknn_index_set_tuning(self._h, mode, byref(Tuning(list_slack, items_per_sm, min_chunk_blocks,
                                                                         bound_refresh, pilot_stride))))
 
+    def apply_tuning(self, mode: int, table: Optional[str] = None) -> int:
+        """Sets the index to the autotuned entry of this device, base size
+        and mode (fknn/autotune.py table), if there is one; returns its k'
+        (0 when there is no entry or the mode is exact)."""
+        from . import autotune
+        e = autotune.lookup(self.n, mode, self.device, table)
+        if not e:
+            return 0
+        t = e["tuning"]
+        self.set_tuning(mode, t["list_slack"], t["items_per_sm"], t["min_chunk_blocks"], t["bound_refresh"],
+                        t["pilot_stride"])
+        return int(e.get("kprime", 0))
+
     def get_tuning(self, mode: int) -> dict:
         t = Tuning()
         check(load().fknn_index_get_tuning(self._h, mode, byref(t)))
