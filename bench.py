@@ -65,6 +65,11 @@ def parse():
     ap.add_argument("--rates", default="10000,50000,200000")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-forms", default="bf16,exact")
+    ap.add_argument("--graph", action="store_true",
+                    help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
+                         "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
+    ap.add_argument("--graph-beams", default="64,128,256,512")
+    ap.add_argument("--graph-cats", type=int, default=8, help="largest categories that get a graph")
     a = ap.parse_args()
     a.kprime_set = a.kprime is not None
     if a.kprime is None:
@@ -375,8 +380,99 @@ def run_serve(args):
     idx.close()
 
 
+def run_graph(args):
+    """Per-category graph search (config-4 generator, Zipf 1.5 over 10,000
+    categories): one graph of out-degree 32 per large category, built by the
+    reference's HNSW::Build (oracle/_ref) over that category's rows; every
+    type-1 query of those categories searches its category's graph with
+    SearchFilter (pool = beam) on the GPU, its refine=min(150, beam)
+    candidates are re-ranked in FP32 on the GPU (fknn_rerank), and recall@100
+    is taken against the exact path's ids.  queries/s counts the graph
+    search plus the re-rank, inputs resident.  The reference Searcher is
+    timed on a sample of the same queries on one host thread."""
+    import ctypes
+
+    import torch
+
+    import fknn
+    import oracle
+    from fknn import datagen
+    torch.cuda.set_device(0)
+    R = oracle.ref_graph()
+    if R is None:
+        print(json.dumps({"mode": "graph", "unavailable": "reference graph build (oracle/_ref/libref_graph.so) not built"}))
+        return
+    n = args.n or 1_000_000
+    nq_all = args.nq or 200_000
+    vecs, labels, ts, q, metas = datagen.make_workload(4, n=n, nq=nq_all)
+    lab = labels.astype(np.int64)
+    counts = np.bincount(lab)
+    cats = np.argsort(-counts, kind="stable")[:args.graph_cats]
+    idx = fknn.Index(vecs, labels, ts)
+    graphs, t_build = {}, 0.0
+    tmp = tempfile.mkdtemp()
+    for c in cats:
+        rows = np.nonzero(lab == c)[0]
+        t0 = time.perf_counter()
+        gb = oracle.ref_hnsw_graph(vecs[rows], ts[rows], 32, 100, os.path.join(tmp, f"g{c}.bin"))
+        t_build += time.perf_counter() - t0
+        graphs[int(c)] = (rows, fknn.GraphSearcher(gb, vecs[rows]), os.path.join(tmp, f"g{c}.bin"))
+    sel = np.nonzero((metas[:, 0] == 1) & np.isin(metas[:, 1].astype(np.int64), cats))[0]
+    qs, ms = q[sel], metas[sel]
+    exact_ids, _ = idx.search(qs, ms, k=100, mode=fknn.MODE_EXACT_FP32)
+    per_cat = {int(c): np.nonzero(ms[:, 1].astype(np.int64) == c)[0] for c in cats}
+    dq = {c: torch.from_numpy(np.ascontiguousarray(qs[ix])).cuda() for c, ix in per_cat.items()}
+    rows_t = {c: torch.from_numpy(graphs[c][0].astype(np.int64)).cuda() for c in per_cat}
+    for beam in [int(b) for b in args.graph_beams.split(",")]:
+        refine = min(150, beam)
+        out = np.full((len(sel), 100), 0xFFFFFFFF, np.uint32)  # beams under 100 return fewer ids
+        for rep in range(2):  # first pass warms up
+            torch.cuda.synchronize()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            res = {}
+            for c, ix in per_cat.items():
+                if len(ix) == 0:
+                    continue
+                loc = graphs[c][1].SearchFilter(dq[c], beam, refine)
+                cand = rows_t[c][loc.long()].to(torch.int32).contiguous()
+                res[c] = idx.rerank(dq[c], cand, k=min(100, refine), with_dists=False)[0]
+            e1.record()
+            torch.cuda.synchronize()
+        ms_gpu = e0.elapsed_time(e1)
+        for c, ix in per_cat.items():
+            if c in res:
+                out[ix, :res[c].shape[1]] = res[c].cpu().numpy().view(np.uint32)
+        rec = datagen.recall_matrix(out, exact_ids)
+        # reference Searcher (mode 1 = SearchFilter) on a sample of the top category's queries, one thread
+        c0 = int(cats[0])
+        smp = per_cat[c0][:min(len(per_cat[c0]), 300)]
+        rows0 = graphs[c0][0]
+        v0, l0, t0_ = vecs[rows0], labels[rows0], ts[rows0]
+        t0 = time.perf_counter()  # graph load + SetData's quantizer training, subtracted below
+        oracle.ref_graph_search(graphs[c0][2], v0, l0, t0_, qs[smp[:1]], 1, beam, refine)
+        t_setup = time.perf_counter() - t0
+        t0 = time.perf_counter()
+        oracle.ref_graph_search(graphs[c0][2], v0, l0, t0_, qs[smp], 1, beam, refine)
+        t_ref = max(1e-9, time.perf_counter() - t0 - t_setup)
+        print(json.dumps({
+            "mode": "graph", "metric": "filtered queries/s, graph beam search + FP32 re-rank", "unit": UNIT,
+            "value": len(sel) / (ms_gpu * 1e-3), "ms": ms_gpu, "beam": beam, "refine": refine,
+            "recall_at_100_vs_exact": rec,
+            "config": {"workload": "uneven-selectivity (config-4 generator)", "n": n, "queries": int(len(sel)),
+                       "query_type": 1, "categories_with_graphs": [int(c) for c in cats],
+                       "category_rows": [int(counts[c]) for c in cats], "out_degree": 32, "ef_construction": 100},
+            "graph_build_s_reference_cpu": t_build,
+            "reference_cpu": {"value": len(smp) / t_ref, "unit": UNIT, "cores": 1, "kind": "reference",
+                              "sample": f"{len(smp)} queries of category {c0} (largest graph), SearchFilter, one thread"},
+        }), flush=True)
+    idx.close()
+
+
 def main():
     args = parse()
+    if args.graph:
+        return run_graph(args)
     if args.sweep:
         return run_sweep(args)
     if args.serve:

@@ -191,6 +191,17 @@ int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoint
 int fknn_sq8_bruteforce_subgraph(size_t dim, size_t k, int *closest_points, float *distances, size_t npoints,
                                  const char *codes_in, float alpha, size_t nqueries, const int8_t *queries_in);
 
+/* FP32 re-rank of candidate lists (hybrid_graph.cpp:216-228, 284-296,
+ * 481-492: approximate candidates re-scored in FP32, the k best kept).
+ * cand is nq x nc ids of index rows in the caller's original numbering
+ * (UINT32_MAX = empty slot; repeats allowed); per query the k smallest
+ * exact distances (normal_l2 arithmetic, distance.h:62-72) are written
+ * ascending by (distance, id), padded with UINT32_MAX / +inf.  The
+ * reference keeps them in heap-array order; the set is the same.  Requires
+ * 1 <= k <= nc <= 2048. */
+int fknn_rerank(fknn_index *index, const float *qvecs, uint32_t nq, const uint32_t *cand, uint32_t nc, uint32_t k,
+                uint32_t *ids, float *dists, void *stream);
+
 /* ---- Graph beam search (pyglass Searcher over an HNSW level-0 graph) ---- */
 
 /* Search forms, numbered as the reference's Searcher methods. */

@@ -167,6 +167,28 @@ class Index:
         check(load().fknn_index_get_tuning(self._h, mode, byref(t)))
         return t.as_dict()
 
+    def rerank(self, qvecs, cand, k: int = K, with_dists: bool = True, stream: Optional[int] = None):
+        """fknn_rerank: the k best of each query's candidate ids (nq, nc)
+        by exact FP32 distance, ascending.  Host arrays in, numpy out; torch
+        CUDA tensors in, torch CUDA tensors out."""
+        dev = _is_torch(qvecs) and qvecs.is_cuda
+        nq, nc = cand.shape
+        if dev:
+            import torch
+            ids = torch.empty((nq, k), dtype=torch.int32, device=qvecs.device)
+            dists = torch.empty((nq, k), dtype=torch.float32, device=qvecs.device) if with_dists else None
+            if stream is None:
+                stream = _stream_of(qvecs)
+        else:
+            qvecs = np.ascontiguousarray(qvecs, dtype=np.float32)
+            cand = np.ascontiguousarray(cand).astype(np.uint32, copy=False)
+            ids = np.empty((nq, k), dtype=np.uint32)
+            dists = np.empty((nq, k), dtype=np.float32) if with_dists else None
+        check(load().fknn_rerank(self._h, _ptr(qvecs, np.float32), nq, _ptr(cand, np.uint32), nc, k,
+                                 _ptr(ids, np.uint32), _ptr(dists, np.float32) if dists is not None else None,
+                                 stream))
+        return ids, dists
+
     def count_matches(self, metas) -> np.ndarray:
         metas = np.ascontiguousarray(metas, dtype=np.float32)
         out = np.empty(metas.shape[0], dtype=np.uint32)
