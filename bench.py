@@ -152,10 +152,10 @@ def fp32_gemm_peak_tflops(torch) -> float:
     return 2 * 8192 ** 3 / (best * 1e-3) / 1e12
 
 
-def traffic_per_pair():
-    """DRAM bytes per screened (query, row) pair of the screening kernel,
+def traffic_per_pair(name: str = "k_screen_traffic.json"):
+    """DRAM bytes per screened (query, row) pair of a screening kernel,
     from the committed ncu summary (None if not measured yet)."""
-    p = os.path.join(ROOT, "profiles", "k_screen_traffic.json")
+    p = os.path.join(ROOT, "profiles", name)
     try:
         with open(p) as f:
             return json.load(f).get("dram_bytes_per_screened_pair")
@@ -608,8 +608,9 @@ def main():
             pairs = st_bf16[-1]["pairs_contraction"]
             ach = 2.0 * 100 * pairs / (ms_s * 1e-3) / 1e12
             pk = peaks.get("bf16_tflops", 1590.0)
-            return {"bound": "tensor", "kernel": "k_screen_bf16", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
-                    "frac": ach / pk, "traffic": None,
+            tpp_tc = traffic_per_pair("k_screen_tc_traffic.json")
+            return {"bound": "tensor", "kernel": "k_screen_tc", "achieved": ach, "peak": pk, "unit": "TFLOP/s",
+                    "frac": ach / pk, "traffic": tpp_tc * st_bf16[-1]["pairs_screened"] if tpp_tc else None,
                     "peak_source": "MEASURED_PEAKS.json bf16_tflops (cuBLAS bf16 burst)" +
                                    (" [fallback]" if peaks.get("fallback") else ""),
                     "algorithmic": "2*d*P flops, d=100, P = passing (query,row) pairs of the contraction's queries",
