@@ -264,6 +264,8 @@ def run_sweep(args):
     n, nq = args.n or w.n, args.nq or w.nq
     vecs, labels, ts, q, metas = datagen.make_workload(args.config, n=n, nq=nq)
     idx = fknn.Index(vecs, labels, ts, build_bf16=True, build_fp8=True)
+    for md in (fknn.MODE_EXACT_FP32, fknn.MODE_BF16_RERANK, fknn.MODE_FP8_RERANK):
+        idx.apply_tuning(md)  # plan / kernel parameters only; k' is swept here
     stream = torch.cuda.current_stream()
     dq, dm = torch.from_numpy(q).cuda(), torch.from_numpy(metas).cuda()
     rng = np.random.default_rng(17)
@@ -337,8 +339,11 @@ def run_serve(args):
     nreq = int(max(rates) * args.serve_seconds) + 1
     vecs, labels, ts, q, metas = datagen.make_workload(cfg, n=n, nq=nreq)
     idx = fknn.Index(vecs, labels, ts, build_bf16=True)
+    idx.apply_tuning(fknn.MODE_EXACT_FP32)
+    kp_tuned = idx.apply_tuning(fknn.MODE_BF16_RERANK)
     exact_ids, _ = idx.search(q, metas, k=100, mode=fknn.MODE_EXACT_FP32)
-    forms = {"bf16": (fknn.MODE_BF16_RERANK, args.kprime), "exact": (fknn.MODE_EXACT_FP32, 0)}
+    kp = args.kprime if args.kprime_set or not kp_tuned else kp_tuned
+    forms = {"bf16": (fknn.MODE_BF16_RERANK, kp), "exact": (fknn.MODE_EXACT_FP32, 0)}
     for fname in args.serve_forms.split(","):
         mode, kp = forms[fname]
         with fknn.Server(idx, mode=mode, kprime=kp, max_batch=4096, slots=3) as srv:
