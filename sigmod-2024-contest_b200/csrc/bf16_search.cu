@@ -835,6 +835,8 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   QueryDesc *d_desc, *h_desc;
   float *h_meta;
   if ((rc = prepare_queries(idx, d_q, d_meta, nq, st, &d_desc, &h_desc, &h_meta))) return rc;
+  uint32_t nsmall_early = 0;
+  if ((rc = launch_small_scans(idx, h_desc, d_desc, nq, d_q, k, d_ids, d_dists, st, &nsmall_early))) return rc;
   const fknn_tuning tune = idx->tuning[F::kFP8 ? FKNN_MODE_FP8_RERANK : FKNN_MODE_BF16_RERANK];
   // candidate slots per (item, query): k' plus the pushes between trims; a
   // list holds at most 1280 (32 lanes x 40 registers in the trim)
@@ -969,12 +971,9 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
     g_launches += 3;
   }
   if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));
-  if (nsmall)
-    if ((rc = launch_exact_scan(idx, (const uint32_t *)(d_blob + o_small), nullptr, nsmall,
-                                std::min<uint32_t>(nsmall, 148 * 8), d_desc, d_q, k, d_ids, d_dists, st)))
-      return rc;
   if (nbig)
     if ((rc = launch_exact_scan(idx, ovf_list, ovf_count, 0, 148 * 2, d_desc, d_q, k, d_ids, d_dists, st))) return rc;
+  if (nsmall_early && (rc = join_small_scans(idx, st))) return rc;
   FKNN_CUDA(cudaGetLastError());
   if (stats) {
     FKNN_CUDA(cudaEventRecord(ev[3], st));

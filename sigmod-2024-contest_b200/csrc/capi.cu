@@ -88,6 +88,9 @@ static void free_index(fknn_index *idx) {
   if (!idx) return;
   cudaSetDevice(idx->device);
   cudaDeviceSynchronize();
+  if (idx->side_stream) cudaStreamDestroy(idx->side_stream);
+  if (idx->ev_fork) cudaEventDestroy(idx->ev_fork);
+  if (idx->ev_join) cudaEventDestroy(idx->ev_join);
   if (idx->is_view) {
     for (auto &b : idx->ws) cudaFree(b.p);
     for (auto &b : idx->hs)
@@ -334,6 +337,8 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     rc = search_fp8(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
   else
     rc = search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
+  // on a failure the short-slab scans may still be writing the outputs
+  if (rc && idx->side_stream) cudaStreamSynchronize(idx->side_stream);
   if (rc) return rc;
   if (!i_dev) FKNN_CUDA(cudaMemcpyAsync(ids, d_ids, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && !dd_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_dists, (size_t)nq * k * 4, cudaMemcpyDeviceToHost, st));

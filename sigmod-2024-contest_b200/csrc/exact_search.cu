@@ -965,6 +965,42 @@ int launch_exact_scan(fknn_index *idx, const uint32_t *list, const uint32_t *d_c
   return FKNN_OK;
 }
 
+// The row-by-row exact scan of every query whose slab has at most
+// SMALL_SLAB rows needs only the slabs, so it starts before the host plan,
+// on the index's side stream (ordered after everything already on st), and
+// runs while the host plans the rest.  Its rows of ids / dists are disjoint
+// from the contraction's.  join_small_scans orders st after it.
+int launch_small_scans(fknn_index *idx, const QueryDesc *h_desc, const QueryDesc *d_desc, uint32_t nq,
+                       const float *d_q, uint32_t k, uint32_t *d_ids, float *d_dists, cudaStream_t st,
+                       uint32_t *nsmall) {
+  int rc;
+  *nsmall = 0;
+  uint32_t *h_list, *d_list;
+  if ((rc = hs_get(idx, 4, (size_t)nq * 4 + 64, (void **)&h_list))) return rc;
+  uint32_t m = 0;
+  for (uint32_t i = 0; i < nq; ++i)
+    if (h_desc[i].e - h_desc[i].s <= (uint32_t)SMALL_SLAB) h_list[m++] = i;
+  *nsmall = m;
+  if (!m) return FKNN_OK;
+  if ((rc = ws_get(idx, 12, (size_t)m * 4 + 64, (void **)&d_list))) return rc;
+  if (!idx->side_stream) FKNN_CUDA(cudaStreamCreateWithFlags(&idx->side_stream, cudaStreamNonBlocking));
+  if (!idx->ev_fork) FKNN_CUDA(cudaEventCreateWithFlags(&idx->ev_fork, cudaEventDisableTiming));
+  if (!idx->ev_join) FKNN_CUDA(cudaEventCreateWithFlags(&idx->ev_join, cudaEventDisableTiming));
+  FKNN_CUDA(cudaEventRecord(idx->ev_fork, st));
+  FKNN_CUDA(cudaStreamWaitEvent(idx->side_stream, idx->ev_fork, 0));
+  FKNN_CUDA(cudaMemcpyAsync(d_list, h_list, (size_t)m * 4, cudaMemcpyHostToDevice, idx->side_stream));
+  if ((rc = launch_exact_scan(idx, d_list, nullptr, m, std::min<uint32_t>(m, 148 * 8), d_desc, d_q, k, d_ids,
+                              d_dists, idx->side_stream)))
+    return rc;
+  FKNN_CUDA(cudaEventRecord(idx->ev_join, idx->side_stream));
+  return FKNN_OK;
+}
+
+int join_small_scans(fknn_index *idx, cudaStream_t st) {
+  if (idx->ev_join) FKNN_CUDA(cudaStreamWaitEvent(st, idx->ev_join, 0));
+  return FKNN_OK;
+}
+
 int launch_fill_u32(uint32_t *p, uint32_t n, uint32_t v, cudaStream_t st) {
   k_fill_u32<<<std::min<uint32_t>((n + 255) / 256, 1024), 256, 0, st>>>(p, n, v);
   g_launches += 1;
@@ -980,6 +1016,8 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
   QueryDesc *d_desc, *h_desc;
   float *h_meta;
   if ((rc = prepare_queries(idx, d_q, d_meta, nq, st, &d_desc, &h_desc, &h_meta))) return rc;
+  uint32_t nsmall_early = 0;
+  if ((rc = launch_small_scans(idx, h_desc, d_desc, nq, d_q, k, d_ids, d_dists, st, &nsmall_early))) return rc;
 
   // 2. plan
   auto t0 = std::chrono::steady_clock::now();
@@ -1078,17 +1116,12 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
     g_launches += 3;
   }
   if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));
-  if (nsmall) {
-    const unsigned grid = std::min<uint32_t>(nsmall, 148 * 8);
-    k_exact_scan<<<grid, ES_THREADS, 0, st>>>((const uint32_t *)(d_blob + o_small), nullptr, nsmall, d_desc, d_q,
-                                              OT.blocks, OC.blocks, OT.perm, OC.perm, k, d_ids, d_dists);
-    g_launches += 1;
-  }
   if (nbig) {
     k_exact_scan<<<148 * 2, ES_THREADS, 0, st>>>(ovf_list, ovf_count, 0, d_desc, d_q, OT.blocks, OC.blocks, OT.perm,
                                                  OC.perm, k, d_ids, d_dists);
     g_launches += 1;
   }
+  if (nsmall_early && (rc = join_small_scans(idx, st))) return rc;
   FKNN_CUDA(cudaGetLastError());
   if (stats) {
     FKNN_CUDA(cudaEventRecord(ev[3], st));

@@ -204,6 +204,9 @@ struct fknn_index {
   fknn::HostBuf hs[8];
   int *d_flag = nullptr;
   cudaStream_t own_stream = nullptr;
+  // side stream of the short-slab scans, which overlap the host plan
+  cudaStream_t side_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   fknn::Plan plan;  // rebuilt by every search; capacity kept
   // per-mode plan / kernel parameters (fknn_index_set_tuning) and the SM count
   fknn_tuning tuning[3] = {{0, 16, 16, 0, 0}, {256, 3, 8, 0, 16}, {256, 3, 8, 0, 16}};
@@ -249,6 +252,10 @@ int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint
 int launch_exact_scan(fknn_index *idx, const uint32_t *list, const uint32_t *d_count, uint32_t h_count, unsigned grid,
                       const QueryDesc *desc, const float *q, uint32_t k, uint32_t *ids, float *dists, cudaStream_t st);
 int launch_fill_u32(uint32_t *p, uint32_t n, uint32_t v, cudaStream_t st);
+int launch_small_scans(fknn_index *idx, const QueryDesc *h_desc, const QueryDesc *d_desc, uint32_t nq,
+                       const float *d_q, uint32_t k, uint32_t *d_ids, float *d_dists, cudaStream_t st,
+                       uint32_t *nsmall);
+int join_small_scans(fknn_index *idx, cudaStream_t st);
 
 // reduced-precision search (bf16_search.cu)
 int build_bf16(fknn_index *idx, cudaStream_t st);
