@@ -119,6 +119,36 @@ __device__ __forceinline__ void tmem_ld32(uint32_t addr, float (&v)[32]) {
   for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
 
+// 64 accumulator columns of this warp's 32 TMEM lanes in one load
+__device__ __forceinline__ void tmem_ld64(uint32_t addr, float (&v)[64]) {
+  uint32_t r[64];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x64.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31,%32,%33,%34,%35,%36,%37,%38,%39,%40,%41,%42,%43,%44,%45,%46,%47,%48,%49,%50,%51,%52,%53,%54,%55,%56,%57,%58,%59,%60,%61,%62,%63}, [%64];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31]), "=r"(r[32]), "=r"(r[33]), "=r"(r[34]), "=r"(r[35]), "=r"(r[36]), "=r"(r[37]), "=r"(r[38]), "=r"(r[39]), "=r"(r[40]), "=r"(r[41]), "=r"(r[42]), "=r"(r[43]), "=r"(r[44]), "=r"(r[45]), "=r"(r[46]), "=r"(r[47]), "=r"(r[48]), "=r"(r[49]), "=r"(r[50]), "=r"(r[51]), "=r"(r[52]), "=r"(r[53]), "=r"(r[54]), "=r"(r[55]), "=r"(r[56]), "=r"(r[57]), "=r"(r[58]), "=r"(r[59]), "=r"(r[60]), "=r"(r[61]), "=r"(r[62]), "=r"(r[63])
+      : "r"(addr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int j = 0; j < 64; ++j) v[j] = __uint_as_float(r[j]);
+}
+
+// max of 32 values as a tree (NaN entries ignored)
+__device__ __forceinline__ float max32(const float *v) {
+  float a[8];
+#pragma unroll
+  for (int k = 0; k < 8; ++k) a[k] = fmaxf(fmaxf(v[4 * k], v[4 * k + 1]), fmaxf(v[4 * k + 2], v[4 * k + 3]));
+  return fmaxf(fmaxf(fmaxf(a[0], a[1]), fmaxf(a[2], a[3])), fmaxf(fmaxf(a[4], a[5]), fmaxf(a[6], a[7])));
+}
+
+// bit j set iff v[j] >= t (false for NaN), built as four independent chains
+__device__ __forceinline__ uint32_t ge_mask32(const float *v, float t) {
+  uint32_t p[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int g = 0; g < 4; ++g) p[g] |= (v[g * 8 + j] >= t ? 1u : 0u) << (g * 8 + j);
+  return (p[0] | p[1]) | (p[2] | p[3]);
+}
+
 __device__ __forceinline__ void mbar_arrive1(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
 }
@@ -550,43 +580,35 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc)
       const float cq = (T == INFINITY) ? -INFINITY : 0.5f * (qn - T) / sc;
 #pragma unroll 1
-      for (int c = 0; c < BR; c += 32) {
-        float v[32];
-        tmem_ld32(tmem + ((uint32_t)(wg * 32) << 16) + ab * BR + c, v);
-        if (r0 >= c + 32 || r1 <= c) continue;
-        float m = -INFINITY;
-        const bool whole = r0 <= c && r1 >= c + 32;
-        if (whole) {
+      for (int c2 = 0; c2 < BR; c2 += 64) {
+        float v[64];
+        tmem_ld64(tmem + ((uint32_t)(wg * 32) << 16) + ab * BR + c2, v);
+        if (r0 >= c2 + 64 || r1 <= c2) continue;
+        if (!(r0 <= c2 && r1 >= c2 + 64)) {
+          // columns outside this query's slab become NaN: ignored by the max, rejected by every compare
 #pragma unroll
-          for (int j = 0; j < 32; ++j) m = fmaxf(m, v[j]);
-        } else {
-#pragma unroll
-          for (int j = 0; j < 32; ++j)
-            if (c + j >= r0 && c + j < r1) m = fmaxf(m, v[j]);
+          for (int j = 0; j < 64; ++j)
+            if (c2 + j < r0 || c2 + j >= r1) v[j] = __int_as_float(0x7fc00000);
         }
-        if (m >= cq) {
-          // this lane's candidates as a bit mask; their values are read back
-          // from shared memory, so the push loop runs once per candidate of
-          // the lane with the most, not once per column
-          uint32_t mask = 0;
-          if (whole) {
 #pragma unroll
-            for (int j = 0; j < 32; ++j) mask |= (v[j] >= cq ? 1u : 0u) << j;
-          } else {
+        for (int h = 0; h < 64; h += 32) {
+          if (max32(v + h) >= cq) {
+            // this lane's candidates as a bit mask; their values are read back
+            // from shared memory, so the push loop runs once per candidate of
+            // the lane with the most, not once per column
+            uint32_t mask = ge_mask32(v + h, cq);
+            float *row = &sm.stage[wslot][lane * STAGE_ROW];
 #pragma unroll
-            for (int j = 0; j < 32; ++j) mask |= (v[j] >= cq && c + j >= r0 && c + j < r1 ? 1u : 0u) << j;
-          }
-          float *row = &sm.stage[wslot][lane * STAGE_ROW];
-#pragma unroll
-          for (int j = 0; j < 32; j += 4)
-            *reinterpret_cast<float4 *>(row + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-          while (mask) {
-            const int j = __ffs(mask) - 1;
-            mask &= mask - 1;
-            Candidate cd;
-            cd.ds = fmaf(-2.f * sc, row[j], qn);
-            cd.pos = p0 + c + j;
-            list[cnt++] = cd;
+            for (int j = 0; j < 32; j += 4)
+              *reinterpret_cast<float4 *>(row + j) = make_float4(v[h + j], v[h + j + 1], v[h + j + 2], v[h + j + 3]);
+            while (mask) {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1;
+              Candidate cd;
+              cd.ds = fmaf(-2.f * sc, row[j], qn);
+              cd.pos = p0 + c2 + h + j;
+              list[cnt++] = cd;
+            }
           }
         }
       }
