@@ -615,24 +615,29 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive1(&sm.accempty[ab]);
-      // lists that could overflow in the next sub-tile are bounded and trimmed
-      sm.cnt[L] = cnt;
-      const bool need = cnt > (int)capb - BR;
-      uint32_t msk = __ballot_sync(0xffffffffu, need);
-      __syncwarp();
-      while (msk) {
-        const int b = __ffs(msk) - 1;
-        msk &= msk - 1;
-        const int Lb = wg * 32 + b;
-        bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+      // lists that could overflow in the next sub-tile are bounded and
+      // trimmed; counts and bounds pass through shared memory only then
+      uint32_t msk = __ballot_sync(0xffffffffu, cnt > (int)capb - BR);
+      if (msk) {
+        sm.cnt[L] = cnt;
+        __syncwarp();
+        while (msk) {
+          const int b = __ffs(msk) - 1;
+          msk &= msk - 1;
+          const int Lb = wg * 32 + b;
+          bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+        }
+        cnt = sm.cnt[L];
+        T = sm.thr[L];
       }
       // other items of the same query tighten the shared bound meanwhile
       if (refresh && sub % refresh == refresh - 1 && qi >= 0) {
         const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
-        if (Tg < sm.thr[L]) sm.thr[L] = Tg;
+        if (Tg < T) {
+          T = Tg;
+          sm.thr[L] = T;
+        }
       }
-      cnt = sm.cnt[L];
-      T = sm.thr[L];
     }
     if (!ok) {
       if (qi >= 0) ovf[qi] = 1u;
@@ -695,14 +700,8 @@ __global__ void __launch_bounds__(RR_THREADS)
   const QueryDesc dsc = desc[qi];
   for (int d = tid; d < DIM; d += RR_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
   // candidate counts of the query's items (a tile has at most a few dozen)
-  if (tid == 0) {
-    uint32_t total = nitems > RR_THREADS ? RR_CAP + 1 : 0;  // more items than prefix slots: exact scan
-    for (uint32_t i = 0; i < nitems && i < RR_THREADS; ++i) {
-      sm.cnt_prefix[i] = total;
-      total += out_cnt[(uint64_t)item_slot[tl.item0 + i] * BQ + L];
-    }
-    sm.total = (int)total;
-  }
+  // more items than prefix slots: the exact scan answers the query
+  list_offsets(item_slot, tl.item0, nitems, out_cnt, L, BQ, sm.cnt_prefix, &sm.total, RR_THREADS, RR_CAP + 1);
   __syncthreads();
   const int M = sm.total;
   // a pilot bound that kept fewer than k' rows was set too low: the exact

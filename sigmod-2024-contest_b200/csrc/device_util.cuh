@@ -193,4 +193,34 @@ __device__ __forceinline__ int sq8_dist(const int *__restrict__ qw, int qq, cons
 }
 
 
+// Offsets of one query's candidate lists in the merge: warp 0 reads the
+// item counts (item_slot[item0 + i] selects the item, lane L of tq the
+// list) 32 at a time and scans them with shuffles.  prefix[i] = first
+// position of item i, *total = their sum, or over_value when there are more
+// than max_items items.  Caller: the whole block, then __syncthreads().
+__device__ __forceinline__ void list_offsets(const uint32_t *__restrict__ item_slot, uint32_t item0, uint32_t nitems,
+                                             const uint32_t *__restrict__ out_cnt, uint32_t L, uint32_t tq,
+                                             uint32_t *prefix, int *total, uint32_t max_items, int over_value) {
+  if (threadIdx.x >= 32) return;
+  const int lane = threadIdx.x;
+  if (nitems > max_items) {
+    if (lane == 0) *total = over_value;
+    return;
+  }
+  uint32_t carry = 0;
+  for (uint32_t base = 0; base < nitems; base += 32) {
+    const uint32_t i = base + lane;
+    const uint32_t c = i < nitems ? out_cnt[(uint64_t)item_slot[item0 + i] * tq + L] : 0u;
+    uint32_t inc = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += v;
+    }
+    if (i < nitems) prefix[i] = carry + inc - c;
+    carry += __shfl_sync(0xffffffffu, inc, 31);
+  }
+  if (lane == 0) *total = (int)carry;
+}
+
 }  // namespace fknn

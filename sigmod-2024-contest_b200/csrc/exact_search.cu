@@ -470,14 +470,8 @@ __global__ void __launch_bounds__(MG_THREADS)
   for (int d = tid; d < DIM; d += MG_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
   // 1. gather the lists: item offsets (a tile has at most a few dozen
   // items), then the whole block copies each list
-  if (tid == 0) {
-    uint32_t total = nitems > MG_THREADS ? MERGE_CAP + 1 : 0;  // more items than offset slots: exact scan
-    for (uint32_t i = 0; i < nitems && i < MG_THREADS; ++i) {
-      sm.cnt_prefix[i] = total;
-      total += out_cnt[(uint64_t)item_slot[tl.item0 + i] * TQ + L];
-    }
-    sm.total = (int)total;
-  }
+  // more items than offset slots: the exact scan answers the query
+  list_offsets(item_slot, tl.item0, nitems, out_cnt, L, TQ, sm.cnt_prefix, &sm.total, MG_THREADS, MERGE_CAP + 1);
   __syncthreads();
   const int M = sm.total;
   if (M > MERGE_CAP) {
