@@ -751,44 +751,73 @@ int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *cou
 // range into row chunks.
 namespace {
 
-// Sorts plan keys by (order, cls, bucket, e, s, qi): an LSD radix sort on
-// the packed 128-bit image (order 1 bit, cls 2, bucket 29, e 32 | s 32, qi
-// 32), 16-bit digits, passes whose digit is constant skipped.
+inline int bits_for(uint64_t v) {
+  int b = 0;
+  while (b < 64 && (v >> b)) ++b;
+  return b;
+}
+
+// Sorts plan keys by (order, cls, bucket, e, s, qi).  The keys arrive in
+// increasing qi and the LSD radix sort is stable, so qi needs no key bits;
+// the other fields are packed into one 64-bit key at their actual widths
+// (49 bits at n = 1e6) and sorted with 11-bit digits, passes whose digit is
+// constant skipped.  Wider packings fall back to two 64-bit words.
 void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
   const size_t m = keys.size();
   if (m < 2) return;
+  uint32_t max_e = 0, max_s = 0, max_b = 0;
+  for (const PlanKey &k : keys) {
+    max_e = std::max(max_e, k.e);
+    max_s = std::max(max_s, k.s);
+    max_b = std::max<uint32_t>(max_b, (uint32_t)std::min<uint64_t>(k.bucket, 0xffffffffu));
+  }
+  const int be = bits_for(max_e), bs = bits_for(max_s), bb = bits_for(max_b);
+  const bool one_word = 3 + bb + be + bs <= 64;
   auto &hi = W.w_hi, &lo = W.w_lo, &hi2 = W.w_hi2, &lo2 = W.w_lo2;
   auto &ix = W.w_ix, &ix2 = W.w_ix2, &cnt = W.w_cnt;
-  hi.resize(m);
   lo.resize(m);
-  hi2.resize(m);
   lo2.resize(m);
   ix.resize(m);
   ix2.resize(m);
-  cnt.resize(65537);
+  if (!one_word) {
+    hi.resize(m);
+    hi2.resize(m);
+  }
   for (size_t i = 0; i < m; ++i) {
     const PlanKey &k = keys[i];
-    hi[i] = ((uint64_t)k.order << 63) | ((uint64_t)(k.cls & 3) << 61) | ((k.bucket & 0x1fffffffull) << 32) | k.e;
-    lo[i] = ((uint64_t)k.s << 32) | k.qi;
+    const uint64_t head = ((uint64_t)k.order << 2) | (k.cls & 3);
+    if (one_word) {
+      lo[i] = (((((head << bb) | k.bucket) << be) | k.e) << bs) | k.s;
+    } else {
+      hi[i] = (head << 61) | ((k.bucket & 0x1fffffffull) << 32) | k.e;
+      lo[i] = k.s;
+    }
     ix[i] = (uint32_t)i;
   }
-  for (int pass = 0; pass < 8; ++pass) {
-    const bool upper = pass >= 4;
-    const int shift = (pass & 3) * 16;
-    const std::vector<uint64_t> &src = upper ? hi : lo;
-    std::fill(cnt.begin(), cnt.end(), 0u);
-    for (size_t i = 0; i < m; ++i) ++cnt[((src[i] >> shift) & 0xffff) + 1];
-    if (cnt[((src[0] >> shift) & 0xffff) + 1] == m) continue;  // one digit value: order unchanged
-    for (int d = 0; d < 65536; ++d) cnt[d + 1] += cnt[d];
-    for (size_t i = 0; i < m; ++i) {
-      const uint32_t pos = cnt[(src[i] >> shift) & 0xffff]++;
-      hi2[pos] = hi[i];
-      lo2[pos] = lo[i];
-      ix2[pos] = ix[i];
+  constexpr int DB = 11, NB = 1 << DB;
+  cnt.resize(NB + 1);
+  const int words = one_word ? 1 : 2;
+  for (int w = 0; w < words; ++w) {
+    const int width = w == 0 ? (one_word ? 3 + bb + be + bs : 32) : 64;
+    for (int shift = 0; shift < width; shift += DB) {
+      std::vector<uint64_t> &src = w == 0 ? lo : hi;
+      std::vector<uint64_t> &dst = w == 0 ? lo2 : hi2;
+      std::fill(cnt.begin(), cnt.end(), 0u);
+      for (size_t i = 0; i < m; ++i) ++cnt[((src[i] >> shift) & (NB - 1)) + 1];
+      if (cnt[((src[0] >> shift) & (NB - 1)) + 1] == m) continue;  // one digit value: order unchanged
+      for (int d = 0; d < NB; ++d) cnt[d + 1] += cnt[d];
+      for (size_t i = 0; i < m; ++i) {
+        const uint32_t pos = cnt[(src[i] >> shift) & (NB - 1)]++;
+        dst[pos] = src[i];
+        ix2[pos] = ix[i];
+        if (w == 0 && !one_word) hi2[pos] = hi[i];
+        if (w == 1) lo2[pos] = lo[i];
+      }
+      src.swap(dst);
+      if (w == 0 && !one_word) hi.swap(hi2);
+      if (w == 1) lo.swap(lo2);
+      ix.swap(ix2);
     }
-    hi.swap(hi2);
-    lo.swap(lo2);
-    ix.swap(ix2);
   }
   auto &out = W.w_keys2;
   out.resize(m);
