@@ -664,38 +664,61 @@ __global__ void __launch_bounds__(B_THREADS, 2)
 // ------------------------------------------------------------ re-rank --
 
 constexpr int RR_THREADS = 256;
-constexpr int RR_CAP = 8192;  // screening candidates one block can hold
-constexpr int RR_KMAX = 1024; // largest k'
+constexpr int RR_CAP = 8192;        // screening candidates the large merge holds
+constexpr int RR_CAP_SMALL = 2048;  // ... and the common one (8 blocks per SM)
+constexpr int RR_KMAX = 1024;       // largest k'
 
+template <int CAP>
 struct RerankSmem {
-  float key[RR_CAP];
-  uint32_t val[RR_CAP];
+  float key[CAP];
+  uint32_t val[CAP];
   uint64_t ekey[RR_KMAX];
   float qv[DIM];
   uint32_t cnt_prefix[RR_THREADS + 1];
   int total;
 };
 
-__global__ void __launch_bounds__(RR_THREADS)
-    k_merge_rerank(const uint32_t *__restrict__ big_q, const uint32_t *__restrict__ big_tile,
-                   const uint32_t *__restrict__ big_lane, const Tile *__restrict__ tiles,
-                   const uint32_t *__restrict__ item_slot, const Candidate *__restrict__ out,
-                   const uint32_t *__restrict__ out_cnt, const QueryDesc *__restrict__ desc,
-                   const float *__restrict__ q, const float *__restrict__ vecs, const uint32_t *__restrict__ perm_t,
-                   const uint32_t *__restrict__ perm_c, const uint32_t *__restrict__ ovf,
-                   uint32_t *__restrict__ ovf_list, uint32_t *__restrict__ ovf_count, uint32_t k, uint32_t kprime,
-                   uint32_t capb, const uint32_t *__restrict__ seeded, uint32_t *__restrict__ ids,
-                   float *__restrict__ dists, uint32_t *__restrict__ n_f64) {
-  extern __shared__ __align__(1024) unsigned char smem_raw[];
-  RerankSmem &sm = *reinterpret_cast<RerankSmem *>(smem_raw);
+struct MergeArgs {
+  const uint32_t *big_q, *big_tile, *big_lane;
+  const Tile *tiles;
+  const uint32_t *item_slot;
+  const Candidate *out;
+  const uint32_t *out_cnt;
+  const QueryDesc *desc;
+  const float *q, *vecs;
+  const uint32_t *perm_t, *perm_c, *ovf;
+  uint32_t *ovf_list, *ovf_count;
+  uint32_t k, kprime, capb;
+  const uint32_t *seeded;
+  uint32_t *ids;
+  float *dists;
+  uint32_t *n_f64;
+};
+
+// One big query b (index into the plan's big-query arrays): gather its
+// lists, keep the k' best screening distances, re-rank them in FP32.  A
+// query with more than CAP candidates goes to `spill` (the large merge) or,
+// from the large merge, to the exact scan.  Returns are block-uniform.
+template <int CAP>
+__device__ void merge_one(const MergeArgs &A, uint32_t b, RerankSmem<CAP> &sm, uint32_t *spill,
+                          uint32_t *spill_count) {
+  const uint32_t *big_tile = A.big_tile, *big_lane = A.big_lane, *item_slot = A.item_slot, *out_cnt = A.out_cnt;
+  const Tile *tiles = A.tiles;
+  const Candidate *out = A.out;
+  const QueryDesc *desc = A.desc;
+  const float *q = A.q, *vecs = A.vecs;
+  const uint32_t *perm_t = A.perm_t, *perm_c = A.perm_c, *seeded = A.seeded;
+  uint32_t *ovf_list = A.ovf_list, *ovf_count = A.ovf_count, *ids = A.ids, *n_f64 = A.n_f64;
+  float *dists = A.dists;
+  const uint32_t k = A.k, kprime = A.kprime, capb = A.capb;
   const int tid = threadIdx.x;
-  const uint32_t qi = big_q[blockIdx.x];
-  if (ovf[qi]) {
+  const uint32_t qi = A.big_q[b];
+  if (A.ovf[qi]) {
     if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
     return;
   }
-  const Tile tl = tiles[big_tile[blockIdx.x]];
-  const uint32_t L = big_lane[blockIdx.x];
+  const Tile tl = tiles[big_tile[b]];
+  const uint32_t L = big_lane[b];
   const uint32_t nitems = tl.item1 - tl.item0;
   const QueryDesc dsc = desc[qi];
   for (int d = tid; d < DIM; d += RR_THREADS) sm.qv[d] = q[(uint64_t)qi * DIM + d];
@@ -704,9 +727,13 @@ __global__ void __launch_bounds__(RR_THREADS)
   list_offsets(item_slot, tl.item0, nitems, out_cnt, L, BQ, sm.cnt_prefix, &sm.total, RR_THREADS, RR_CAP + 1);
   __syncthreads();
   const int M = sm.total;
+  if (M > CAP && spill && M <= RR_CAP) {  // the large merge takes it
+    if (tid == 0) spill[atomicAdd(spill_count, 1u)] = b;
+    return;
+  }
   // a pilot bound that kept fewer than k' rows was set too low: the exact
   // scan answers the query
-  if (M > RR_CAP || (seeded && seeded[qi] && M < (int)kprime)) {
+  if (M > CAP || (seeded && seeded[qi] && M < (int)kprime)) {
     if (tid == 0) ovf_list[atomicAdd(ovf_count, 1u)] = qi;
     return;
   }
@@ -790,6 +817,22 @@ __global__ void __launch_bounds__(RR_THREADS)
     }
     ids[(uint64_t)qi * k + j] = id;
     if (dists) dists[(uint64_t)qi * k + j] = d;
+  }
+}
+
+// work == nullptr: block b merges big query b (grid = number of big
+// queries); else the blocks stride over the *work_count entries of work.
+template <int CAP>
+__global__ void __launch_bounds__(RR_THREADS)
+    k_merge_rerank(MergeArgs A, uint32_t nbig, const uint32_t *__restrict__ work,
+                   const uint32_t *__restrict__ work_count, uint32_t *__restrict__ spill,
+                   uint32_t *__restrict__ spill_count) {
+  extern __shared__ __align__(1024) unsigned char smem_raw[];
+  RerankSmem<CAP> &sm = *reinterpret_cast<RerankSmem<CAP> *>(smem_raw);
+  const uint32_t nwork = work ? *work_count : nbig;
+  for (uint32_t w = blockIdx.x; w < nwork; w += gridDim.x) {
+    merge_one<CAP>(A, work ? work[w] : w, sm, spill, spill_count);
+    __syncthreads();  // shared memory is reused by the next query
   }
 }
 
@@ -917,12 +960,13 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   put(o_slot, slot.data(), nitems * 4);
   if (blob) FKNN_CUDA(cudaMemcpyAsync(d_blob, h_blob, blob, cudaMemcpyHostToDevice, st));
   uint32_t *d_state;
-  if ((rc = ws_get(idx, 5, (size_t)nq * 12 + 64, (void **)&d_state))) return rc;
+  if ((rc = ws_get(idx, 5, (size_t)nq * 16 + 64, (void **)&d_state))) return rc;
   uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
-           *ovf_count = d_state + 3 * (size_t)nq, *n_f64 = ovf_count + 1;
+           *ovf_count = d_state + 3 * (size_t)nq, *n_f64 = ovf_count + 1, *spill_count = ovf_count + 2;
+  // spill list (big-query indices for the large merge): spill_count + 1 .. + nq
   if ((rc = launch_fill_u32(T_global, nq, f32_sortable(INFINITY), st))) return rc;
   FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
-  FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 8, st));
+  FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 12, st));
   // pilot state: bound estimate, seeded flag, pilot overflow per query
   uint32_t *d_pilot = nullptr, *seeded = nullptr;
   if (tune.pilot_stride > 1) {
@@ -955,8 +999,10 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
                 : capb <= 1024 ? k_screen_tc<F, 32> : k_screen_tc<F, 40>;
     FKNN_CUDA(cudaFuncSetAttribute(screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                    (int)sizeof(BScreenSmem<F>)));
-    FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                   (int)sizeof(RerankSmem)));
+    FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank<RR_CAP_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(RerankSmem<RR_CAP_SMALL>)));
+    FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank<RR_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(RerankSmem<RR_CAP>)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
     void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
     const uint32_t stride = tune.pilot_stride;
@@ -984,12 +1030,36 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
         d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->d_flag);
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
-    k_merge_rerank<<<nbig, RR_THREADS, sizeof(RerankSmem), st>>>(
-        (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
-        (const Tile *)(d_blob + o_tiles), (const uint32_t *)(d_blob + o_slot), d_out, d_ocnt, d_desc, d_q, idx->vecs,
-        OT.perm, OC.perm, ovf, ovf_list, ovf_count, k, kprime, capb, stride > 1 ? seeded : nullptr, d_ids, d_dists,
-        n_f64);
-    g_launches += 3;
+    MergeArgs A;
+    A.big_q = (const uint32_t *)(d_blob + o_big);
+    A.big_tile = (const uint32_t *)(d_blob + o_btile);
+    A.big_lane = (const uint32_t *)(d_blob + o_blane);
+    A.tiles = (const Tile *)(d_blob + o_tiles);
+    A.item_slot = (const uint32_t *)(d_blob + o_slot);
+    A.out = d_out;
+    A.out_cnt = d_ocnt;
+    A.desc = d_desc;
+    A.q = d_q;
+    A.vecs = idx->vecs;
+    A.perm_t = OT.perm;
+    A.perm_c = OC.perm;
+    A.ovf = ovf;
+    A.ovf_list = ovf_list;
+    A.ovf_count = ovf_count;
+    A.k = k;
+    A.kprime = kprime;
+    A.capb = capb;
+    A.seeded = stride > 1 ? seeded : nullptr;
+    A.ids = d_ids;
+    A.dists = d_dists;
+    A.n_f64 = n_f64;
+    // queries with more candidates than the common merge holds go to the large one
+    uint32_t *spill = spill_count + 1;
+    k_merge_rerank<RR_CAP_SMALL><<<nbig, RR_THREADS, sizeof(RerankSmem<RR_CAP_SMALL>), st>>>(
+        A, nbig, nullptr, nullptr, spill, spill_count);
+    k_merge_rerank<RR_CAP><<<148 * 2, RR_THREADS, sizeof(RerankSmem<RR_CAP>), st>>>(A, 0, spill, spill_count,
+                                                                                     nullptr, nullptr);
+    g_launches += 4;
   }
   if (stats) FKNN_CUDA(cudaEventRecord(ev[2], st));
   if (nbig)
