@@ -75,6 +75,7 @@ struct GParams {
   uint32_t nq;
   int mode;
   uint32_t cap, refine;
+  bool batch;  // refine <= cap: the overflow slot is never read, inserts may be batched
   const float *bounds;
   const int32_t *id_bounds;
   int32_t *out_ids;
@@ -89,6 +90,7 @@ struct Warp {
   Slot *pool;
   uint32_t *chg;   // block flags [2][nblkw]
   int *qw;         // query code as 28 words
+  int *cand;       // sorted candidate distances of a batch insert (32)
   uint64_t *mass;  // bitmaps [2][nwords]
   int qq;
   uint32_t size, cur;
@@ -99,7 +101,7 @@ __host__ __device__ inline size_t pool_bytes(uint32_t cap) {
 }
 
 __host__ __device__ inline size_t warp_smem_bytes(uint32_t cap, uint32_t nblkw) {
-  return pool_bytes(cap) + 2 * (size_t)nblkw * 4 + CODE;
+  return pool_bytes(cap) + 2 * (size_t)nblkw * 4 + CODE + 32 * sizeof(int);
 }
 
 __device__ __forceinline__ int gdist(const GParams &P, const Warp &W, uint32_t v) {
@@ -204,14 +206,83 @@ __device__ __forceinline__ Chunk load_chunk(const int32_t *list, uint32_t len, u
   return c;
 }
 
+// The lanes of mask m inserted one after another in lane order, in one
+// pass over the pool.  Equal distances keep insertion order (the pool's
+// upper-bound rule: old entries first, then candidates by lane), so the
+// pool's first cap slots, its size and its cursor end as after the one-by-one
+// inserts: the pool is the first cap entries of the stable merge, and the
+// cursor moves to the first candidate's final slot.  Only the overflow slot
+// (slot cap) is not kept, so this is used when it is never read.
+__device__ void pool_insert_batch(Warp &W, uint32_t cap, uint32_t m, int v, int d) {
+  const int lane = threadIdx.x & 31;
+  const int n = __popc(m);
+  // warp bitonic sort of the keys (distance, lane); empty lanes sort last
+  uint32_t key = (m >> lane) & 1u ? ((uint32_t)d << 5) | (uint32_t)lane : 0xffffffffu;
+#pragma unroll
+  for (int size = 2; size <= 32; size <<= 1)
+#pragma unroll
+    for (int stride = size >> 1; stride > 0; stride >>= 1) {
+      const uint32_t other = __shfl_xor_sync(0xffffffffu, key, stride);
+      const bool asc = (lane & size) == 0, lower = (lane & stride) == 0;
+      key = (lower == asc) ? min(key, other) : max(key, other);
+    }
+  const int cd = (int)(key >> 5);
+  const int cv = __shfl_sync(0xffffffffu, v, (int)(key & 31));
+  if (lane < n) W.cand[lane] = cd;
+  __syncwarp();
+  // candidate j's final slot: j + pool entries with distance <= d_j
+  uint32_t pos = 0xffffffffu;
+  if (lane < n) {
+    uint32_t lo = 0, hi = W.size;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (W.pool[mid].d > cd) hi = mid;
+      else lo = mid + 1;
+    }
+    pos = (uint32_t)lane + lo;
+  }
+  const uint32_t first = __shfl_sync(0xffffffffu, pos, 0);  // entries below it do not move
+  // old entry i moves up by the number of candidates strictly closer, top chunk first
+  for (int top = (int)W.size - 1; top >= (int)first; top -= 32) {
+    const int i = top - lane;
+    Slot t;
+    int ni = (int)cap;
+    if (i >= (int)first) {
+      t = W.pool[i];
+      int a = 0, b = n;
+      while (a < b) {
+        const int mid = (a + b) >> 1;
+        if (W.cand[mid] < t.d) a = mid + 1;
+        else b = mid;
+      }
+      ni = i + a;
+    }
+    __syncwarp();
+    if (ni < (int)cap) W.pool[ni] = t;
+    __syncwarp();
+  }
+  if (pos < cap) {
+    Slot sl;
+    sl.d = cd;
+    sl.id = cv;
+    W.pool[pos] = sl;
+  }
+  __syncwarp();
+  W.size = min(W.size + (uint32_t)n, cap);
+  if (first < cap && first < W.cur) W.cur = first;
+}
+
 // Inserts the lanes of mask m in lane order (the adjacency order).
-__device__ __forceinline__ int insert_lanes(Warp &W, uint32_t cap, uint32_t m, int v, int d) {
-  int count = 0;
+__device__ __forceinline__ int insert_lanes(const GParams &P, Warp &W, uint32_t m, int v, int d) {
+  const int count = __popc(m);
+  if (P.batch && count > 1) {
+    pool_insert_batch(W, P.cap, m, v, d);
+    return count;
+  }
   while (m) {
     const int b = __ffs(m) - 1;
     m &= m - 1;
-    pool_insert(W, cap, __shfl_sync(0xffffffffu, v, b), __shfl_sync(0xffffffffu, d, b));
-    ++count;
+    pool_insert(W, P.cap, __shfl_sync(0xffffffffu, v, b), __shfl_sync(0xffffffffu, d, b));
   }
   return count;
 }
@@ -227,7 +298,7 @@ __device__ void expand_plain(const GParams &P, Warp &W, uint32_t u) {
     const bool fresh = c.valid && c.first && !vis_get(P, W, 0, (uint32_t)c.v);
     const int d = fresh ? gdist(P, W, (uint32_t)c.v) : 0;
     vis_set(P, W, 0, (uint32_t)c.v, fresh);
-    insert_lanes(W, P.cap, __ballot_sync(0xffffffffu, fresh), c.v, d);
+    insert_lanes(P, W, __ballot_sync(0xffffffffu, fresh), c.v, d);
     if (c.end) break;
   }
 }
@@ -251,7 +322,7 @@ __device__ void expand_filtered(const GParams &P, Warp &W, uint32_t u, float l, 
     const int d = pass ? gdist(P, W, (uint32_t)c.v) : 0;
     vis_set(P, W, 0, (uint32_t)c.v, fresh);
     count2 += __popc(__ballot_sync(0xffffffffu, fresh));
-    count1 += insert_lanes(W, P.cap, __ballot_sync(0xffffffffu, pass), c.v, d);
+    count1 += insert_lanes(P, W, __ballot_sync(0xffffffffu, pass), c.v, d);
     if (c.end) break;
   }
   for (uint32_t i = 0; i < P.K; ++i) {
@@ -282,7 +353,7 @@ __device__ void expand_filtered(const GParams &P, Warp &W, uint32_t u, float l, 
       const bool mine = (upto >> lane) & 1u;
       const int d = (pass && mine) ? gdist(P, W, (uint32_t)c.v) : 0;
       vis_set(P, W, 0, (uint32_t)c.v, fresh && mine);
-      count1 += insert_lanes(W, P.cap, passm & upto, c.v, d);
+      count1 += insert_lanes(P, W, passm & upto, c.v, d);
       if (stop || c.end) break;
     }
   }
@@ -353,6 +424,7 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_graph_search(GParams P) {
   W.pool = reinterpret_cast<Slot *>(mine);
   W.chg = reinterpret_cast<uint32_t *>(mine + pool_bytes(P.cap));
   W.qw = reinterpret_cast<int *>(W.chg + 2 * P.nblkw);
+  W.cand = W.qw + 28;
   const uint32_t slot = blockIdx.x * GS_WARPS + wib;
   W.mass = P.vis + (uint64_t)slot * 2 * P.nwords;
   for (uint32_t qi = slot; qi < P.nq; qi += gridDim.x * GS_WARPS) {
@@ -705,6 +777,7 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
   P.mode = mode;
   P.cap = cap;
   P.refine = refine;
+  P.batch = refine <= cap;
   P.bounds = ranged ? b_use : nullptr;
   P.id_bounds = ranged ? ib_use : nullptr;
   P.out_ids = ids_use;
