@@ -503,8 +503,8 @@ def main():
     nq = args.nq or w.nq
     vecs, labels, ts = datagen.make_base(n, w.zipf_s, w.n_labels, 1234 + args.config)
     # every rank its own query batch (weak scaling); rank 0 = the workload's queries
-    q, metas = datagen.make_queries(nq, w.zipf_s, w.n_labels, w.window, w.balanced_types, 1234 + args.config,
-                                    1235 + args.config + 1000 * rank)
+    from fknn import replicas
+    q, metas = replicas.rank_queries(args.config, nq, rank)
     idx = fknn.Index(vecs, labels, ts, device=local, build_bf16=True)
     # autotuned plan / kernel parameters and k' for this device and base size, if recorded
     idx.apply_tuning(fknn.MODE_EXACT_FP32)
@@ -523,11 +523,7 @@ def main():
         torch.cuda.synchronize()
 
     def max_over_ranks(x):
-        if world > 1:
-            t = torch.tensor([x], device="cuda")
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            return float(t.item())
-        return x
+        return replicas.max_over_ranks(x, "cuda")
 
     def timed(mode, kprime, out_ids):
         """W untimed steps, then K steps between barriers, CUDA events on the
@@ -559,7 +555,7 @@ def main():
     use_bf16 = recall_bf16 >= 0.99
     head_mode = fknn.MODE_BF16_RERANK if use_bf16 else fknn.MODE_EXACT_FP32
     ms = ms_bf16 if use_bf16 else ms_exact
-    value = world * nq / (ms * 1e-3)
+    value = replicas.job_value(world, nq, ms)
 
     # correctness spot check of the exact path (not timed): 64 queries vs the oracle
     check = None

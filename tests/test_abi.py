@@ -71,3 +71,25 @@ def test_no_cpu_fallback_without_a_device():
     assert e.value.code == _lib.FKNN_ENODEV
     with pytest.raises(fknn.FknnError):
         fknn.Bruteforce(np.zeros((8, 102), np.float32), np.zeros((1, 104), np.float32))
+
+
+def test_graph_and_server_arguments_are_checked_without_a_device():
+    """Malformed Graph::save bytes are rejected while parsing (before any
+    device work); the request loop and the re-rank reject NULL arguments."""
+    lib = fknn.load()
+    vec = np.zeros((4, 100), dtype=np.float32)
+    h = c_void_p()
+    bad = np.array([0, 4, 2, 1, 2, -1, -1, 0, 0, 0, 0, 0, 0], dtype=np.int32)  # no eps, no initializer
+    assert lib.fknn_graph_create(bad.ctypes.data, bad.nbytes, vec.ctypes.data, 0, byref(h)) == fknn.FKNN_EINVAL
+    assert b"Graph::save" in lib.fknn_last_error()
+    trunc = np.array([1, 0, 4, 2], dtype=np.int32)  # adjacency missing
+    assert lib.fknn_graph_create(trunc.ctypes.data, trunc.nbytes, vec.ctypes.data, 0, byref(h)) == fknn.FKNN_EINVAL
+    oob = np.concatenate([np.array([1, 0, 2, 1], np.int32), np.array([5, 0], np.int32),
+                          np.zeros(2, np.float32).view(np.int32)])  # neighbour id 5 of a 2-point graph
+    assert lib.fknn_graph_create(oob.ctypes.data, oob.nbytes, vec.ctypes.data, 0, byref(h)) == fknn.FKNN_EINVAL
+    assert lib.fknn_graph_search(None, None, 1, 0, 10, 0, 10, None, None, None, None, None) == fknn.FKNN_EINVAL
+    assert lib.fknn_server_create(None, None, byref(h)) == fknn.FKNN_EINVAL
+    assert lib.fknn_server_submit(None, None, None, 1, None, None, None, None) == fknn.FKNN_EINVAL
+    assert lib.fknn_rerank(None, None, 1, None, 10, 5, None, None, None) == fknn.FKNN_EINVAL
+    t = _lib.Tuning(100, 0, 0, 0, 0)  # list_slack below 256
+    assert lib.fknn_index_set_tuning(None, 1, byref(t)) == fknn.FKNN_EINVAL
