@@ -22,6 +22,8 @@
 // normal_l2's exact operation sequence and ordered by (dist, id) like the
 // ResultMaxHeap of utils.h:35-78.
 #include <algorithm>
+#include <functional>
+#include <thread>
 #include <chrono>
 #include <cmath>
 #include <cstring>
@@ -757,24 +759,23 @@ inline int bits_for(uint64_t v) {
   return b;
 }
 
-// Sorts plan keys by (order, cls, bucket, e, s, qi).  The keys arrive in
-// increasing qi and the LSD radix sort is stable, so qi needs no key bits;
-// the other fields are packed into one 64-bit key at their actual widths
-// (49 bits at n = 1e6) and sorted with 11-bit digits, passes whose digit is
-// constant skipped.  Wider packings fall back to two 64-bit words.
-void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
-  const size_t m = keys.size();
+// Sorts keys[0..m) of one query class by (bucket, e, s, qi).  The keys
+// arrive in increasing qi and the LSD radix sort is stable, so qi needs no
+// key bits; bucket, e and s are packed into one 64-bit key at their actual
+// widths (under 49 bits at n = 1e6) and sorted with 11-bit digits, passes
+// whose digit is constant skipped.  Wider packings use two 64-bit words.
+void sort_class(PlanKey *keys, size_t m, Plan::SortScratch &W) {
   if (m < 2) return;
   uint32_t max_e = 0, max_s = 0, max_b = 0;
-  for (const PlanKey &k : keys) {
-    max_e = std::max(max_e, k.e);
-    max_s = std::max(max_s, k.s);
-    max_b = std::max<uint32_t>(max_b, (uint32_t)std::min<uint64_t>(k.bucket, 0xffffffffu));
+  for (size_t i = 0; i < m; ++i) {
+    max_e = std::max(max_e, keys[i].e);
+    max_s = std::max(max_s, keys[i].s);
+    max_b = std::max<uint32_t>(max_b, (uint32_t)std::min<uint64_t>(keys[i].bucket, 0xffffffffu));
   }
   const int be = bits_for(max_e), bs = bits_for(max_s), bb = bits_for(max_b);
-  const bool one_word = 3 + bb + be + bs <= 64;
-  auto &hi = W.w_hi, &lo = W.w_lo, &hi2 = W.w_hi2, &lo2 = W.w_lo2;
-  auto &ix = W.w_ix, &ix2 = W.w_ix2, &cnt = W.w_cnt;
+  const bool one_word = bb + be + bs <= 64;
+  auto &hi = W.hi, &lo = W.lo, &hi2 = W.hi2, &lo2 = W.lo2;
+  auto &ix = W.ix, &ix2 = W.ix2, &cnt = W.cnt;
   lo.resize(m);
   lo2.resize(m);
   ix.resize(m);
@@ -785,11 +786,10 @@ void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
   }
   for (size_t i = 0; i < m; ++i) {
     const PlanKey &k = keys[i];
-    const uint64_t head = ((uint64_t)k.order << 2) | (k.cls & 3);
     if (one_word) {
-      lo[i] = (((((head << bb) | k.bucket) << be) | k.e) << bs) | k.s;
+      lo[i] = ((((uint64_t)k.bucket << be) | k.e) << bs) | k.s;
     } else {
-      hi[i] = (head << 61) | ((k.bucket & 0x1fffffffull) << 32) | k.e;
+      hi[i] = ((k.bucket & 0xffffffffull) << 32) | k.e;
       lo[i] = k.s;
     }
     ix[i] = (uint32_t)i;
@@ -798,7 +798,7 @@ void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
   cnt.resize(NB + 1);
   const int words = one_word ? 1 : 2;
   for (int w = 0; w < words; ++w) {
-    const int width = w == 0 ? (one_word ? 3 + bb + be + bs : 32) : 64;
+    const int width = w == 0 ? (one_word ? bb + be + bs : 32) : 64;
     for (int shift = 0; shift < width; shift += DB) {
       std::vector<uint64_t> &src = w == 0 ? lo : hi;
       std::vector<uint64_t> &dst = w == 0 ? lo2 : hi2;
@@ -819,10 +819,39 @@ void sort_keys(std::vector<PlanKey> &keys, Plan &W) {
       ix.swap(ix2);
     }
   }
-  auto &out = W.w_keys2;
+  auto &out = W.out;
   out.resize(m);
   for (size_t i = 0; i < m; ++i) out[i] = keys[ix[i]];
-  keys.swap(out);
+  std::copy(out.begin(), out.end(), keys);
+}
+
+// Sorts plan keys by (order, cls, bucket, e, s, qi): a stable partition by
+// class in (order, cls) order -- classes 0 and 2 on the time order, then 1
+// and 3 on the category order -- and the classes' own sorts side by side
+// on host threads.  Class 0 (no predicate) needs none: its keys are equal.
+void sort_keys(std::vector<PlanKey> &keys, Plan &P) {
+  const size_t m = keys.size();
+  if (m < 2) return;
+  static const int rank_of_cls[4] = {0, 2, 1, 3};  // (order, cls) order of the classes
+  size_t start[5] = {0, 0, 0, 0, 0};
+  for (const PlanKey &k : keys) ++start[rank_of_cls[k.cls & 3] + 1];
+  for (int r = 0; r < 4; ++r) start[r + 1] += start[r];
+  auto &part = P.w_keys2;
+  part.resize(m);
+  size_t fill[4] = {start[0], start[1], start[2], start[3]};
+  for (const PlanKey &k : keys) part[fill[rank_of_cls[k.cls & 3]]++] = k;
+  keys.swap(part);
+  std::vector<std::thread> pool;
+  for (int r = 1; r < 4; ++r) {
+    const size_t len = start[r + 1] - start[r];
+    if (len < 2) continue;
+    if (len < 4096 || pool.size() == 2) {
+      sort_class(keys.data() + start[r], len, P.w_sort[r]);
+    } else {
+      pool.emplace_back(sort_class, keys.data() + start[r], len, std::ref(P.w_sort[r]));
+    }
+  }
+  for (auto &t : pool) t.join();
 }
 
 }  // namespace

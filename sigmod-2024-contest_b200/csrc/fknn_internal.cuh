@@ -130,9 +130,14 @@ struct Plan {
   std::vector<int32_t> lane_q;
   std::vector<uint32_t> lane_s, lane_e;
   uint64_t pairs_screened = 0, pairs_passing = 0, pairs_contraction = 0;
-  // working storage
-  std::vector<uint32_t> w_big, w_ix, w_ix2, w_cnt, w_per_tile, w_slot, w_fill;
-  std::vector<uint64_t> w_hi, w_lo, w_hi2, w_lo2;
+  // working storage; the sort of each query class has its own
+  struct SortScratch {
+    std::vector<uint32_t> ix, ix2, cnt;
+    std::vector<uint64_t> hi, lo, hi2, lo2;
+    std::vector<PlanKey> out;
+  };
+  SortScratch w_sort[4];
+  std::vector<uint32_t> w_big, w_per_tile, w_slot, w_fill;
   std::vector<PlanKey> w_keys, w_keys2;
   std::vector<PlanTile> w_tiles;
   std::vector<WorkItem> w_items;
