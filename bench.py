@@ -66,6 +66,9 @@ def parse():
     ap.add_argument("--rates", default="10000,50000,200000")
     ap.add_argument("--serve-seconds", type=float, default=2.0)
     ap.add_argument("--serve-forms", default="bf16,exact")
+    ap.add_argument("--filter", action="store_true",
+                    help="predicate-compaction run instead of the headline: fknn_filter_rows over the base for a "
+                         "sample of the workload's predicates; HBM GB/s of algorithmic bytes")
     ap.add_argument("--graph", action="store_true",
                     help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
                          "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
@@ -475,8 +478,59 @@ def run_graph(args):
     idx.close()
 
 
+def run_filter(args):
+    """fknn_filter_rows (the predicate + compaction kernels) on the resident
+    columns: per call the algorithmic bytes are 8 B per row (int32 label +
+    float32 timestamp) plus 4 B per passing row written; time by CUDA events
+    around the call on its stream (the call also reads the count back)."""
+    import ctypes
+
+    import torch
+
+    import fknn
+    from fknn import _lib, datagen
+    torch.cuda.set_device(0)
+    w = datagen.WORKLOADS[args.config]
+    n = args.n or w.n
+    vecs, labels, ts, q, metas = datagen.make_workload(args.config, n=n, nq=64)
+    idx = fknn.Index(vecs, labels, ts)
+    lib = _lib.load()
+    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    cnt = ctypes.c_uint64()
+    rows = []
+    for i in range(metas.shape[0]):
+        m4 = np.ascontiguousarray(metas[i], dtype=np.float32)
+        for rep in range(args.warmup + args.steps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(stream)
+            _lib.check(lib.fknn_filter_rows(idx._h, m4.ctypes.data, out.data_ptr(), ctypes.byref(cnt),
+                                            stream.cuda_stream))
+            e1.record(stream)
+            e1.synchronize()
+            if rep >= args.warmup:
+                rows.append((int(m4[0]), int(cnt.value), e0.elapsed_time(e1)))
+    ms = np.array([r[2] for r in rows])
+    byts = np.array([8.0 * n + 4.0 * r[1] for r in rows])
+    gbs = byts.sum() / (ms.sum() * 1e-3) / 1e9
+    peaks = measured_peaks()
+    pk = peaks.get("hbm_gbs", 6650.0)
+    per_type = {t: float(np.mean([r[2] for r in rows if r[0] == t])) for t in range(4) if any(r[0] == t for r in rows)}
+    print(json.dumps({"mode": "filter", "metric": "predicate compaction HBM GB/s (algorithmic bytes)",
+                      "value": gbs, "unit": "GB/s", "peak": pk, "frac": gbs / pk,
+                      "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" [fallback]" if peaks.get("fallback") else ""),
+                      "config": {"workload": w.name, "n": n, "predicates": int(metas.shape[0]),
+                                 "calls": len(rows)},
+                      "ms_per_call_mean": float(ms.mean()), "ms_per_call_by_type": per_type,
+                      "algorithmic": "8 B per row (label + timestamp) + 4 B per passing row",
+                      "passing_rows_mean": float(np.mean([r[1] for r in rows]))}), flush=True)
+    idx.close()
+
+
 def main():
     args = parse()
+    if args.filter:
+        return run_filter(args)
     if args.graph:
         return run_graph(args)
     if args.sweep:

@@ -651,44 +651,98 @@ __global__ void k_filter_count(const float *__restrict__ labels, const float *__
 }
 
 // Pass 2 (after an exclusive scan of tile_cnt): write passing ids in order.
+// Each thread keeps its 16 predicates as a bit mask; one block scan over the
+// (item, warp) counts gives every ballot its output offset.
 __global__ void k_filter_write(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n, float4 m,
                                const uint32_t *__restrict__ tile_off, uint32_t *__restrict__ out) {
-  __shared__ uint32_t wcnt[FC_THREADS / 32];
-  __shared__ uint32_t run;
+  constexpr int NW = FC_THREADS / 32;
+  __shared__ uint32_t cnt[FC_ITEMS * NW + 1];
   const uint32_t type = (uint32_t)m.x;
   const int32_t v = (int32_t)m.y;
   const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
   const uint64_t base = (uint64_t)blockIdx.x * FC_TILE;
-  if (threadIdx.x == 0) run = tile_off[blockIdx.x];
-  __syncthreads();
+  uint32_t bits = 0, ballots[FC_ITEMS];
+#pragma unroll
   for (int i = 0; i < FC_ITEMS; ++i) {
     const uint64_t idx = base + (uint64_t)i * FC_THREADS + threadIdx.x;
     const bool p = idx < n && row_passes(type, v, m.z, m.w, labels[idx], ts[idx]);
-    const uint32_t b = __ballot_sync(0xffffffffu, p);
-    if (lane == 0) wcnt[w] = __popc(b);
-    __syncthreads();
-    uint32_t before = run;
-    for (int ww = 0; ww < w; ++ww) before += wcnt[ww];
-    if (p) out[before + __popc(b & ((1u << lane) - 1u))] = (uint32_t)idx;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-      uint32_t s = 0;
-      for (int ww = 0; ww < FC_THREADS / 32; ++ww) s += wcnt[ww];
-      run += s;
-    }
-    __syncthreads();
+    ballots[i] = __ballot_sync(0xffffffffu, p);
+    bits |= (p ? 1u : 0u) << i;
   }
+  // counts in output order: item-major, then warp
+  if (lane < FC_ITEMS) {
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < FC_ITEMS; ++i)
+      if (i == lane) c = __popc(ballots[i]);
+    cnt[lane * NW + w] = c;
+  }
+  __syncthreads();
+  if (threadIdx.x < 32) {  // exclusive scan of the FC_ITEMS * NW = 128 counts, 4 per lane
+    constexpr int PER = FC_ITEMS * NW / 32;
+    uint32_t loc[PER], sum = 0;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      loc[j] = cnt[lane * PER + j];
+      sum += loc[j];
+    }
+    uint32_t inc = sum;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    uint32_t run = tile_off[blockIdx.x] + inc - sum;
+#pragma unroll
+    for (int j = 0; j < PER; ++j) {
+      cnt[lane * PER + j] = run;
+      run += loc[j];
+    }
+  }
+  __syncthreads();
+  const uint32_t lt = (1u << lane) - 1u;
+#pragma unroll
+  for (int i = 0; i < FC_ITEMS; ++i)
+    if ((bits >> i) & 1u)
+      out[cnt[i * NW + w] + __popc(ballots[i] & lt)] = (uint32_t)(base + (uint64_t)i * FC_THREADS + threadIdx.x);
 }
 
-__global__ void k_exclusive_scan_small(uint32_t *data, uint32_t len, uint32_t *total) {
-  // single thread; len is N/4096 (a few thousand)
-  uint32_t s = 0;
-  for (uint32_t i = 0; i < len; ++i) {
-    uint32_t v = data[i];
-    data[i] = s;
-    s += v;
+// Exclusive scan of the tile counts in place, one block; *total = their sum.
+__global__ void __launch_bounds__(1024) k_exclusive_scan_small(uint32_t *data, uint32_t len, uint32_t *total) {
+  __shared__ uint32_t wsum[32];
+  __shared__ uint32_t carry;
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (uint32_t base = 0; base < len; base += blockDim.x) {
+    const uint32_t i = base + threadIdx.x;
+    const uint32_t v = i < len ? data[i] : 0u;
+    uint32_t inc = v;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, inc, o);
+      if (lane >= o) inc += t;
+    }
+    if (lane == 31) wsum[w] = inc;
+    __syncthreads();
+    if (w == 0) {
+      const uint32_t x = lane < (int)(blockDim.x >> 5) ? wsum[lane] : 0u;
+      uint32_t y = x;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t t = __shfl_up_sync(0xffffffffu, y, o);
+        if (lane >= o) y += t;
+      }
+      wsum[lane] = y - x;  // exclusive sum of the warps before
+    }
+    __syncthreads();
+    const uint32_t c = carry;
+    if (i < len) data[i] = c + wsum[w] + inc - v;
+    __syncthreads();
+    if (threadIdx.x == blockDim.x - 1) carry = c + wsum[w] + inc;
+    __syncthreads();
   }
-  *total = s;
+  if (threadIdx.x == 0) *total = carry;
 }
 
 __global__ void k_fill_u32(uint32_t *__restrict__ p, uint32_t n, uint32_t v) {
@@ -738,7 +792,7 @@ int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *cou
   if (rc) return rc;
   const float4 m = make_float4(m4[0], m4[1], m4[2], m4[3]);
   k_filter_count<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc);
-  k_exclusive_scan_small<<<1, 1, 0, st>>>(tc, ntiles, tc + ntiles);
+  k_exclusive_scan_small<<<1, 1024, 0, st>>>(tc, ntiles, tc + ntiles);
   k_filter_write<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc, d_out);
   g_launches += 3;
   uint32_t tot = 0;
@@ -1293,7 +1347,7 @@ extern "C" int fknn_filter_rows_noalloc(const float *labels, const float *ts, ui
   // every tile counter and the total are rewritten by this call, so nothing
   // left in the array by an earlier call is read
   k_filter_count<<<ntiles, FC_THREADS, 0, st>>>(labels, ts, n, m, tc);
-  k_exclusive_scan_small<<<1, 1, 0, st>>>(tc, ntiles, tc + ntiles);
+  k_exclusive_scan_small<<<1, 1024, 0, st>>>(tc, ntiles, tc + ntiles);
   k_filter_write<<<ntiles, FC_THREADS, 0, st>>>(labels, ts, n, m, tc, out_ids);
   g_launches += 3;
   FKNN_CUDA(cudaGetLastError());

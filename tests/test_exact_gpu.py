@@ -142,6 +142,26 @@ def test_filter_rows_compaction():
             np.testing.assert_array_equal(got, np.nonzero(keep)[0].astype(np.uint32))
 
 
+def test_filter_rows_many_tiles():
+    """More tiles than one scan block holds (4.5M rows = 1,099 tiles of 4,096)."""
+    n = 4_500_000
+    rng = np.random.default_rng(3)
+    labels = rng.integers(0, 50, n).astype(np.float32)
+    ts = rng.random(n, dtype=np.float32)
+    vecs = np.zeros((n, 100), np.float32)
+    with fknn.Index(vecs, labels, ts) as idx:
+        for m in (np.array([0, 0, 0, 0], np.float32), np.array([1, 7, 0, 0], np.float32),
+                  np.array([2, 0, 0.25, 0.5], np.float32), np.array([3, 7, 0.1, 0.9], np.float32)):
+            got = idx.filter_rows(m)
+            t = int(m[0])
+            keep = np.ones(n, bool)
+            if t in (1, 3):
+                keep &= labels.astype(np.int32) == np.int32(m[1])
+            if t in (2, 3):
+                keep &= (ts >= m[2]) & (ts <= m[3])
+            np.testing.assert_array_equal(got, np.nonzero(keep)[0].astype(np.uint32))
+
+
 def test_invalid_queries_rejected():
     vecs, labels, ts, q, metas = datagen.make_workload(1, n=5000, nq=4)
     with fknn.Index(vecs, labels, ts) as idx:
