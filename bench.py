@@ -69,6 +69,9 @@ def parse():
     ap.add_argument("--filter", action="store_true",
                     help="predicate-compaction run instead of the headline: fknn_filter_rows over the base for a "
                          "sample of the workload's predicates; HBM GB/s of algorithmic bytes")
+    ap.add_argument("--sq8", action="store_true",
+                    help="SQ8 slab brute force instead of the headline (bruteforce.h:244 with K'=140): codes/s and "
+                         "GB/s over a slab of 4.5 %% of N=1e7 codes, batched queries")
     ap.add_argument("--graph", action="store_true",
                     help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
                          "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
@@ -527,8 +530,84 @@ def run_filter(args):
     idx.close()
 
 
+def run_sq8(args):
+    """fknn_sq8_bruteforce_subgraph over one slab of symmetric SQ8 codes (the
+    reference's brute-force leg for selective queries, hybrid_graph.cpp:206-211
+    and :406-410, K' = 140 in heap-array order), device-resident codes and
+    queries, nq queries per call.  Algorithmic bytes: 112 B per (query, code)
+    pair read; the slab (50 MB) stays in L2 across the queries of a call."""
+    import torch
+
+    import fknn
+    from fknn import _lib, datagen
+    torch.cuda.set_device(0)
+    w = datagen.WORKLOADS[3]
+    npoints = args.n or 450_000
+    nq = args.nq or 2048
+    vecs, labels, ts = datagen.make_base(npoints, w.zipf_s, w.n_labels, 1237)
+    q, _ = datagen.make_queries(nq, w.zipf_s, w.n_labels, w.window, w.balanced_types, 1237, 1238)
+    quant = fknn.SQ8SymmetricQuantizer(100)
+    quant.train(vecs)
+    codes = torch.from_numpy(quant.codes).cuda()
+    qc = torch.from_numpy(quant.encode(q)).cuda()
+    k = 140
+    ids = torch.empty((nq, k), dtype=torch.int32, device="cuda")
+    dd = torch.empty((nq, k), dtype=torch.float32, device="cuda")
+    lib = _lib.load()
+    import ctypes
+
+    def call():
+        _lib.check(lib.fknn_sq8_bruteforce_subgraph(100, k, ids.data_ptr(), dd.data_ptr(), npoints, codes.data_ptr(),
+                                                    ctypes.c_float(quant.alpha), nq, qc.data_ptr()))
+    for _ in range(args.warmup):
+        call()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        call()
+    torch.cuda.synchronize()
+    sec = (time.perf_counter() - t0) / args.steps
+    pairs = nq * npoints
+    line = {"mode": "sq8", "metric": "SQ8 slab brute force, codes scanned per second",
+            "value": pairs / sec, "unit": "codes/s", "gbs_algorithmic": pairs * 112 / sec / 1e9,
+            "ms_per_call": sec * 1e3, "queries_per_s": nq / sec,
+            "config": {"slab_codes": npoints, "queries_per_call": nq, "k": k, "code_bytes": 112}}
+    # The reference's own bruteforce() (compiled from its sources) on the
+    # host cores, one query per call as hybrid_graph.cpp:211 calls it, over a
+    # sample of the same queries; its heap-array ids must equal ours.
+    if not args.no_cpu_baseline:
+        import concurrent.futures as cf
+
+        import oracle as orc
+        ref = orc.ref_sq8()
+        kind = "reference" if ref is not None else "port"
+        codes_h = np.ascontiguousarray(quant.codes)
+        qc_h = np.ascontiguousarray(quant.encode(q))
+        sample = min(nq, args.cpu_sample)
+        out = np.empty((sample, k), dtype=np.int32)
+
+        def one(i):
+            if ref is not None:
+                ref.ref_sq8_bruteforce(k, out[i].ctypes.data, npoints, codes_h.ctypes.data, quant.alpha,
+                                       qc_h[i].ctypes.data)
+            else:
+                out[i] = orc.sq8_bruteforce(k, codes_h, quant.alpha, qc_h[i])
+        cores = os.cpu_count() or 1
+        t0 = time.perf_counter()
+        with cf.ThreadPoolExecutor(cores) as ex:
+            list(ex.map(one, range(sample)))
+        cs = time.perf_counter() - t0
+        got = ids[:sample].cpu().numpy()
+        line["cpu_baseline"] = {"value": sample * npoints / cs, "unit": "codes/s", "cores": cores, "kind": kind,
+                                "sample": f"{sample} queries x {npoints} codes"}
+        line["ids_equal_reference"] = bool((got == out).all())
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
+    if args.sq8:
+        return run_sq8(args)
     if args.filter:
         return run_filter(args)
     if args.graph:

@@ -3,23 +3,19 @@
 //
 // bruteforce() returns the reference's maxPQIFCS heap array, which depends
 // on the exact insertion history (ties on the int distance are frequent).
-// The kernel reproduces it: one block per query scans the slab in chunks of
-// 1024 codes; every code whose distance is below the heap root at the start
-// of its chunk (the only ones must_pop_emplace can admit, since the root
-// only falls) is compacted in slab order with warp ballots and replayed on a
-// shared-memory copy of the heap by one thread, with the reference's
-// emplace / push_down steps.  The distance itself is an exact int32
-// sum over 112 bytes from dp4a: |q-c|^2 = |q|^2 + |c|^2 - 2 q.c.
-#include "device_util.cuh"
+// The kernels below reproduce that history (the three steps are described
+// above k_sq8_prefix).  Every distance is an exact int32 L2SqrSQ8_sym value:
+// |q-c|^2 = |q|^2 + |c|^2 - 2 q.c, from dp4a or from the int8 tensor cores.
+#include <climits>
+#include <mutex>
+
+#include "tc_util.cuh"
 
 namespace fknn {
 
 namespace {
 
 constexpr int SQ8_CODE = 112;
-constexpr int SQ8_WORDS = SQ8_CODE / 4;
-constexpr int BF_THREADS = 256;
-constexpr int BF_CHUNK = 1024;
 constexpr int BF_KMAX = 2048;
 
 __global__ void k_absmax(const float *__restrict__ x, uint64_t count, uint32_t *__restrict__ out) {
@@ -54,105 +50,455 @@ struct HeapNode {
   int id;
 };
 
-// maxPQIFCS::push_down (bruteforce.h:78-87) on a 1-based array.
-__device__ __forceinline__ void heap_push_down(HeapNode *h, int cnt, int x) {
+// ------------------------------------------------------------------------
+// The slab brute force as three steps per batch of queries:
+//
+//  1. k_sq8_prefix (one warp per query): the first SQ_PREFIX codes replayed
+//     exactly -- emplace of the first k, then must_pop_emplace -- with a
+//     warp-wide filter in front of the serial heap steps.  The heap root
+//     afterwards, T_q, bounds every later root (the root only falls), so a
+//     later code can enter only if its distance is below T_q.
+//  2. k_sq8_screen (tcgen05, kind::i8): the int32 inner products of a tile of
+//     128 queries with the code tiles of one slab segment, exact in the
+//     accumulator; an epilogue thread per query writes every code of the
+//     segment with d = |q|^2 + |c|^2 - 2 q.c < T_q, in slab order, to the
+//     query's list for that segment.  A list that fills up marks the query.
+//  3. k_sq8_tail (one warp per query): the heap from step 1, the segment lists
+//     in order through the same filter and serial steps, the heap array out.
+//     A marked query scans the codes itself instead, with the step-1 code.
+//
+// Every distance is the exact int32 L2SqrSQ8_sym value and every code that
+// can enter the heap reaches the serial steps in slab order, so the heap
+// array is the reference's.
+constexpr uint32_t SQ_PREFIX = 8192;    // codes replayed before the screen (multiple of 128)
+constexpr int SQ_WARPS = 4;             // queries per block of the replay kernels
+constexpr int SQ_SCAN = 128;            // codes per warp step of the replay kernels
+constexpr uint32_t SQ_TILE = TC_ROWS * 128;  // 128 rows x 128 bytes (112 code bytes, 16 zero)
+constexpr int SQ_BS = 4;                // shared-memory stages of code tiles
+constexpr int SQ_EPI_WARPS = 4;
+constexpr int SQ_THREADS = (2 + SQ_EPI_WARPS) * 32;  // producer, MMA issuer, epilogue
+constexpr uint32_t SQ_TMEM_COLS = 2 * TC_ROWS;       // double-buffered accumulator
+constexpr int SQ_MMAS = 128 / 32;       // kind::i8: K = 32 bytes per MMA
+constexpr int SQ_NCC_PAD = INT_MIN / 2;  // -|c|^2 of rows past the slab: no candidate test passes
+constexpr uint32_t SQ_QBATCH = 8192;    // queries per pass (bounds the candidate lists)
+// S32 accumulate, signed 8-bit A and B, K-major, N = 128, M = 128
+constexpr uint32_t SQ_IDESC =
+    (2u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(TC_ROWS >> 3) << 17) | ((uint32_t)(TC_ROWS >> 4) << 24);
+
+// code p (row p of 112 bytes; row 0 when p >= bound) as seven 16-byte words
+__device__ __forceinline__ void load_code(const int8_t *__restrict__ codes, uint64_t p, uint64_t bound,
+                                          int4 (&c)[7]) {
+  const int4 *src = reinterpret_cast<const int4 *>(codes + (p < bound ? p : 0) * SQ8_CODE);
+#pragma unroll
+  for (int w = 0; w < 7; ++w) c[w] = __ldg(src + w);
+}
+
+__device__ __forceinline__ int dot112(const int4 (&c)[7], const int4 (&q)[7]) {
+  int s = 0;
+#pragma unroll
+  for (int w = 0; w < 7; ++w) {
+    s = __dp4a(q[w].x, c[w].x, s);
+    s = __dp4a(q[w].y, c[w].y, s);
+    s = __dp4a(q[w].z, c[w].z, s);
+    s = __dp4a(q[w].w, c[w].w, s);
+  }
+  return s;
+}
+
+// Heap steps of maxPQIFCS on a 1-based array, with a hole moved in place of
+// the reference's swaps (the same comparisons, so the same array).
+
+// emplace (bruteforce.h:106-113) at position now (1-based, = new size)
+__device__ __forceinline__ void heap_emplace(HeapNode *h, int now, HeapNode nd) {
+  while (now != 1) {
+    const HeapNode p = h[now >> 1];
+    if (!(nd.d > p.d)) break;
+    h[now] = p;
+    now >>= 1;
+  }
+  h[now] = nd;
+}
+
+// must_pop_emplace (bruteforce.h:99-105) behind the root test
+// bruteforce.h:258-260 makes; push_down (bruteforce.h:78-87) reads both
+// children of a level with one 16-byte load (h is 16-byte aligned and the
+// pair h[2x], h[2x+1] lies inside the heap's region even when 2x = cnt).
+__device__ __forceinline__ void heap_offer(HeapNode *h, int cnt, HeapNode nd) {
+  if (h[1].d <= nd.d) return;
+  int x = 1;
   while ((x << 1) <= cnt) {
-    int t = x << 1;
-    if ((t | 1) <= cnt && h[t | 1].d > h[t].d) t |= 1;
-    if (h[t].d <= h[x].d) break;
-    HeapNode s = h[x];
-    h[x] = h[t];
-    h[t] = s;
+    const int t0 = x << 1;
+    const int4 pr = *reinterpret_cast<const int4 *>(h + t0);
+    int t = t0;
+    HeapNode c;
+    c.d = pr.x;
+    c.id = pr.y;
+    if (t0 + 1 <= cnt && pr.z > pr.x) {
+      t = t0 + 1;
+      c.d = pr.z;
+      c.id = pr.w;
+    }
+    if (c.d <= nd.d) break;
+    h[x] = c;
     x = t;
+  }
+  h[x] = nd;
+}
+
+// nodes of one warp's shared-memory region: the heap (1-based, k + 1 nodes,
+// rounded up to an even count past k + 1 for the pair loads), then the stage
+__host__ __device__ __forceinline__ uint32_t sq_region(uint32_t k) { return ((k + 2u + 1u) & ~1u) + SQ_SCAN; }
+
+// list[0..n) (shared memory) offered in order by lane 0
+__device__ __forceinline__ void offer_list(HeapNode *h, int cnt, const HeapNode *list, int n, int lane) {
+  if (lane == 0)
+    for (int j = 0; j < n; ++j) heap_offer(h, cnt, list[j]);
+  __syncwarp();
+}
+
+// Codes [p0, p1) of the slab through one query's heap, in order: positions
+// below k are emplaced, the rest offered.  The warp scores SQ_SCAN codes per
+// step; lane 0 runs the heap steps for the ones that can enter: all of a step
+// that starts before the heap holds k nodes, else those below the root at the
+// start of the step (the root only falls).  cc[p] = |c_p|^2 = -ncc[p].
+__device__ void scan_codes(HeapNode *heap, HeapNode *stage, const int4 (&qv)[7], int qq,
+                           const int8_t *__restrict__ codes, const int *__restrict__ ncc, uint64_t p0, uint64_t p1,
+                           uint32_t k, int lane) {
+  const uint32_t below = (1u << lane) - 1u;
+  for (uint64_t base = p0; base < p1; base += SQ_SCAN) {
+    int d[SQ_SCAN / 32];
+    int4 c[SQ_SCAN / 32][7];
+#pragma unroll
+    for (int i = 0; i < SQ_SCAN / 32; ++i) load_code(codes, base + 32 * i + lane, p1, c[i]);
+#pragma unroll
+    for (int i = 0; i < SQ_SCAN / 32; ++i) {
+      const uint64_t p = base + 32 * i + lane;
+      d[i] = p < p1 ? qq - ncc[p] - 2 * dot112(c[i], qv) : INT_MAX;
+    }
+    const bool full = base >= k;  // the heap holds k nodes from here on
+    const int root = heap[1].d;
+    int off = 0;
+#pragma unroll
+    for (int i = 0; i < SQ_SCAN / 32; ++i) {
+      const uint64_t p = base + 32 * i + lane;
+      const uint32_t m = __ballot_sync(0xffffffffu, p < p1 && (!full || d[i] < root));
+      if ((m >> lane) & 1u) {
+        HeapNode nd;
+        nd.d = d[i];
+        nd.id = (int)p;
+        stage[off + __popc(m & below)] = nd;
+      }
+      off += __popc(m);
+    }
+    __syncwarp();
+    if (full) {
+      offer_list(heap, (int)k, stage, off, lane);
+    } else {
+      if (lane == 0)
+        for (int j = 0; j < off; ++j) {
+          const HeapNode nd = stage[j];
+          if ((uint32_t)nd.id < k) heap_emplace(heap, nd.id + 1, nd);
+          else heap_offer(heap, (int)k, nd);
+        }
+      __syncwarp();
+    }
   }
 }
 
-__global__ void __launch_bounds__(BF_THREADS)
-    k_sq8_bruteforce(const int8_t *__restrict__ codes, uint64_t npoints, const int8_t *__restrict__ queries,
-                     uint32_t k, int *__restrict__ closest, float *__restrict__ dists, float alpha) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  HeapNode *heap = reinterpret_cast<HeapNode *>(smem_raw);  // [k + 1], 1-based
-  HeapNode *list = heap + (k + 1);                          // [BF_CHUNK]
-  __shared__ int qw[SQ8_WORDS];
-  __shared__ int qq_s;
-  __shared__ uint32_t wcount[BF_THREADS / 32];
-  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t qi = blockIdx.x;
-  const int8_t *q = queries + (uint64_t)qi * SQ8_CODE;
-  if (tid < SQ8_WORDS) qw[tid] = reinterpret_cast<const int *>(q)[tid];
-  __syncthreads();
-  if (tid == 0) {
-    int s = 0;
-    for (int w = 0; w < SQ8_WORDS; ++w) s = __dp4a(qw[w], qw[w], s);
-    qq_s = s;
+__device__ __forceinline__ void load_query(const int8_t *__restrict__ queries, uint32_t q, int4 (&qv)[7], int &qq) {
+  const int4 *src = reinterpret_cast<const int4 *>(queries + (uint64_t)q * SQ8_CODE);
+#pragma unroll
+  for (int w = 0; w < 7; ++w) qv[w] = __ldg(src + w);
+  qq = dot112(qv, qv);
+}
+
+// closest_points[k - l - 1] = data_[l + 1].id (bruteforce.h:262-264), and for
+// bruteforce_subgraph distances[k - l - 1] = data_[l + 1].dist * alpha^2
+__device__ __forceinline__ void write_heap(const HeapNode *heap, uint32_t k, uint64_t q, int *__restrict__ closest,
+                                           float *__restrict__ dists, float alpha, int lane) {
+  for (uint32_t l = lane; l < k; l += 32) {
+    closest[q * k + (k - l - 1)] = heap[l + 1].id;
+    if (dists) dists[q * k + (k - l - 1)] = (float)heap[l + 1].d * alpha * alpha;
   }
-  __syncthreads();
-  const int qq = qq_s;
-  // the first k codes are emplaced unconditionally, in order (bruteforce.h:256-257)
-  for (uint32_t base = 0; base < k; base += BF_CHUNK) {
-    const uint32_t m = min((uint32_t)BF_CHUNK, k - base);
-    for (uint32_t j = tid; j < m; j += BF_THREADS) {
-      list[j].d = sq8_dist(qw, qq, codes + (uint64_t)(base + j) * SQ8_CODE);
-      list[j].id = (int)(base + j);
+}
+
+// Rows [row0, row0 + 128 * ntiles) of n rows of 112 bytes as 128-row
+// core-matrix tiles of 128 bytes per row (bytes 112..127 and rows past n
+// zero), and ncc[r] = -|row r|^2 (SQ_NCC_PAD past n).  One block per tile.
+__global__ void __launch_bounds__(256) k_sq8_tiles(const int8_t *__restrict__ rows, uint64_t n, uint64_t row0,
+                                                   unsigned char *__restrict__ tiles, int *__restrict__ ncc) {
+  const uint64_t t = blockIdx.x;
+  unsigned char *o = tiles + t * SQ_TILE;
+  for (uint32_t c = threadIdx.x; c < TC_ROWS * 8; c += blockDim.x) {
+    const uint32_t r = c >> 3, kc = c & 7;
+    const uint64_t p = row0 + t * TC_ROWS + r;
+    int4 v = make_int4(0, 0, 0, 0);
+    if (kc < 7 && p < n) v = __ldg(reinterpret_cast<const int4 *>(rows + p * SQ8_CODE) + kc);
+    *reinterpret_cast<int4 *>(o + cm_byte(r, kc * 16)) = v;
+  }
+  for (uint32_t r = threadIdx.x; r < (uint32_t)TC_ROWS; r += blockDim.x) {
+    const uint64_t p = row0 + t * TC_ROWS + r;
+    int v = SQ_NCC_PAD;
+    if (p < n) {
+      int4 c[7];
+      load_code(rows, p, n, c);
+      v = -dot112(c, c);
     }
-    __syncthreads();
-    if (tid == 0) {
-      for (uint32_t j = 0; j < m; ++j) {
-        int now = (int)(base + j) + 1;  // maxPQIFCS::emplace (bruteforce.h:106-113)
-        heap[now] = list[j];
-        while (now != 1 && heap[now].d > heap[now >> 1].d) {
-          HeapNode s = heap[now];
-          heap[now] = heap[now >> 1];
-          heap[now >> 1] = s;
-          now >>= 1;
+    ncc[t * TC_ROWS + r] = v;
+  }
+}
+
+// Step 1.  With final set (the whole slab is the prefix) it writes the
+// answer; else the heap and its root T_q.
+__global__ void __launch_bounds__(SQ_WARPS * 32, 4)
+    k_sq8_prefix(const int8_t *__restrict__ codes, const int *__restrict__ ncc, uint64_t prefix,
+                 const int8_t *__restrict__ queries, uint32_t nq, uint32_t k, int final, HeapNode *__restrict__ heaps,
+                 int *__restrict__ T, int *__restrict__ closest, float *__restrict__ dists, float alpha) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t q = blockIdx.x * SQ_WARPS + warp;
+  if (q >= nq) return;  // warp-uniform; the kernel has no block barrier
+  HeapNode *heap = reinterpret_cast<HeapNode *>(smem_raw) + (size_t)warp * sq_region(k);
+  HeapNode *stage = heap + (sq_region(k) - SQ_SCAN);
+  int4 qv[7];
+  int qq;
+  load_query(queries, q, qv, qq);
+  scan_codes(heap, stage, qv, qq, codes, ncc, 0, prefix, k, lane);
+  if (final) {
+    write_heap(heap, k, q, closest, dists, alpha, lane);
+  } else {
+    for (uint32_t l = lane; l <= k; l += 32) heaps[(uint64_t)q * (k + 1) + l] = heap[l];
+    if (lane == 0) T[q] = heap[1].d;
+  }
+}
+
+constexpr int SQ_STAGE_ROW = 36;  // ints per lane row of the candidate staging area
+
+struct SqScreenSmem {
+  unsigned char a[SQ_TILE];
+  unsigned char b[SQ_BS][SQ_TILE];
+  // per epilogue lane, the 32 values y of a chunk that holds candidates
+  // (rows padded to 36 ints: conflict-free 16-byte stores)
+  int stage[SQ_EPI_WARPS][32 * SQ_STAGE_ROW];
+  uint64_t full[SQ_BS], empty[SQ_BS], accfull[2], accempty[2], abar;
+  uint32_t tmem_base;
+};
+static_assert(sizeof(SqScreenSmem) <= 113 * 1024, "two screen CTAs per SM");
+
+__device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t db, uint32_t accumulate) {
+  asm volatile(
+      "{\n .reg .pred p;\n setp.ne.b32 p, %4, 0;\n"
+      " tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n}\n" ::"r"(tmem_d),
+      "l"(da), "l"(db), "r"(SQ_IDESC), "r"(accumulate));
+}
+
+// Step 2.  Block (query tile, segment); the segment is code tiles
+// [seg * tps, min(nct, (seg + 1) * tps)) of the screened part, whose tile t
+// holds slab rows row0 + 128 t ...  The list of query q for segment seg is
+// cand[(q * nseg + seg) * cap ...], its length counts[q * nseg + seg].
+__global__ void __launch_bounds__(SQ_THREADS, 2)
+    k_sq8_screen(const unsigned char *__restrict__ qtiles, const int *__restrict__ qncc, uint32_t nq,
+                 const unsigned char *__restrict__ ctiles, const int *__restrict__ cncc, uint32_t nct, uint32_t tps,
+                 uint32_t nseg, uint32_t row0, const int *__restrict__ T, int2 *__restrict__ cand, uint32_t cap,
+                 uint32_t *__restrict__ counts, uint32_t *__restrict__ mark, int *err) {
+  extern __shared__ __align__(1024) unsigned char screen_smem[];
+  SqScreenSmem &sm = *reinterpret_cast<SqScreenSmem *>(screen_smem);
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  const uint32_t qt = blockIdx.x, seg = blockIdx.y;
+  const uint32_t t0 = seg * tps;
+  const uint32_t ntile = t0 < nct ? min(tps, nct - t0) : 0u;
+
+  if (tid == 0) {
+    for (int s = 0; s < SQ_BS; ++s) {
+      mbar_init(&sm.full[s], 1);
+      mbar_init(&sm.empty[s], 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(&sm.accfull[a], 1);
+      mbar_init(&sm.accempty[a], SQ_EPI_WARPS);
+    }
+    mbar_init(&sm.abar, 1);
+    fence_mbar_init();
+  }
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&sm.tmem_base)),
+                 "r"(SQ_TMEM_COLS));
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = sm.tmem_base;
+
+  if (warp == 0) {
+    // ------------------------------------------------ producer
+    if (lane == 0) {
+      mbar_arrive_expect_tx(&sm.abar, SQ_TILE);
+      bulk_g2s(sm.a, qtiles + (uint64_t)qt * SQ_TILE, SQ_TILE, &sm.abar);
+      uint32_t issued = 0;
+      for (uint32_t sub = 0; sub < ntile; ++sub) {
+        const int st = sub % SQ_BS;
+        if (sub >= SQ_BS && !mbar_wait_bounded(&sm.empty[st], ((sub / SQ_BS) - 1) & 1, err)) break;
+        mbar_arrive_expect_tx(&sm.full[st], SQ_TILE);
+        bulk_g2s(sm.b[st], ctiles + (uint64_t)(t0 + sub) * SQ_TILE, SQ_TILE, &sm.full[st]);
+        ++issued;
+      }
+      // no copy may still be landing when the block exits
+      mbar_wait_bounded(&sm.abar, 0, err);
+      for (uint32_t i = issued > SQ_BS ? issued - SQ_BS : 0; i < issued; ++i)
+        mbar_wait_bounded(&sm.full[i % SQ_BS], (i / SQ_BS) & 1, err);
+    }
+  } else if (warp == 1) {
+    // ------------------------------------------------ MMA issuer
+    if (lane == 0) {
+      uint32_t done = 0;
+      if (mbar_wait_bounded(&sm.abar, 0, err)) {
+        const uint32_t a0 = smem_u32(sm.a);
+        for (uint32_t sub = 0; sub < ntile; ++sub) {
+          const int st = sub % SQ_BS, ab = sub & 1;
+          if (!mbar_wait_bounded(&sm.full[st], (sub / SQ_BS) & 1, err)) break;
+          if (sub >= 2 && !mbar_wait_bounded(&sm.accempty[ab], ((sub >> 1) - 1) & 1, err)) break;
+          tc_fence_after();
+          const uint32_t b0 = smem_u32(sm.b[st]);
+#pragma unroll
+          for (int kk = 0; kk < SQ_MMAS; ++kk) {
+            const uint64_t da = umma_desc(a0 + kk * 2 * (TC_ROWS / 8) * 128, (TC_ROWS / 8) * 128, 128);
+            const uint64_t db = umma_desc(b0 + kk * 2 * (TC_ROWS / 8) * 128, (TC_ROWS / 8) * 128, 128);
+            umma_i8(tmem + ab * TC_ROWS, da, db, kk > 0);
+          }
+          umma_commit(&sm.empty[st]);
+          umma_commit(&sm.accfull[ab]);
+          ++done;
         }
       }
+      // no MMA may be in flight when TMEM is released
+      if (done) mbar_wait_bounded(&sm.accfull[(done - 1) & 1], ((done - 1) >> 1) & 1, err);
     }
-    __syncthreads();
-  }
-  // the rest: must_pop_emplace (bruteforce.h:99-105) through the root filter
-  for (uint64_t base = k; base < npoints; base += BF_CHUNK) {
-    const int root = heap[1].d;
-    uint32_t run = 0;
-    for (int r = 0; r < BF_CHUNK / BF_THREADS; ++r) {
-      const uint64_t p = base + (uint64_t)r * BF_THREADS + tid;
-      int d = 0;
-      bool keep = false;
-      if (p < npoints) {
-        d = sq8_dist(qw, qq, codes + p * SQ8_CODE);
-        keep = d < root;
+  } else {
+    // ------------------------------------------------ epilogue: thread = query
+    const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
+    const uint32_t q = qt * TC_ROWS + wg * 32 + lane;
+    const bool valid = q < nq;
+    // candidate iff d = qq - y < T with y = 2 q.c - |c|^2, i.e. y > qq - T
+    const int qq = valid ? -qncc[q] : 0;
+    const int thr = valid ? qq - T[q] : INT_MAX;
+    int2 *list = cand + ((uint64_t)(valid ? q : 0) * nseg + seg) * cap;
+    int *row = &sm.stage[wg][lane * SQ_STAGE_ROW];
+    uint32_t cnt = 0;
+    bool ok = true;
+    for (uint32_t sub = 0; sub < ntile; ++sub) {
+      const int ab = sub & 1;
+      if (!mbar_wait_bounded(&sm.accfull[ab], (sub >> 1) & 1, err)) {
+        ok = false;
+        break;
       }
-      const uint32_t b = __ballot_sync(0xffffffffu, keep);
-      if (lane == 0) wcount[warp] = __popc(b);
-      __syncthreads();
-      uint32_t before = run;
-      for (int w = 0; w < warp; ++w) before += wcount[w];
-      if (keep) {
-        HeapNode nd;
-        nd.d = d;
-        nd.id = (int)p;
-        list[before + __popc(b & ((1u << lane) - 1u))] = nd;
+      tc_fence_after();
+      const uint32_t tile = t0 + sub;
+      const int *nc = cncc + (uint64_t)tile * TC_ROWS;
+      const int id0 = (int)(row0 + tile * TC_ROWS);
+#pragma unroll 1
+      for (int c2 = 0; c2 < TC_ROWS; c2 += 64) {
+        float v[64];
+        tmem_ld64(tmem + ((uint32_t)(wg * 32) << 16) + ab * TC_ROWS + c2, v);
+#pragma unroll
+        for (int h = 0; h < 64; h += 32) {
+          // y for 32 columns and the candidate bits, four independent chains
+          int y[32];
+          uint32_t mk[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+          for (int j = 0; j < 32; j += 4) {
+            const int4 n4 = __ldg(reinterpret_cast<const int4 *>(nc + c2 + h + j));
+            y[j] = 2 * __float_as_int(v[h + j]) + n4.x;
+            y[j + 1] = 2 * __float_as_int(v[h + j + 1]) + n4.y;
+            y[j + 2] = 2 * __float_as_int(v[h + j + 2]) + n4.z;
+            y[j + 3] = 2 * __float_as_int(v[h + j + 3]) + n4.w;
+#pragma unroll
+            for (int g = 0; g < 4; ++g) mk[g] |= (y[j + g] > thr ? 1u : 0u) << (j + g);
+          }
+          uint32_t mask = (mk[0] | mk[1]) | (mk[2] | mk[3]);
+          if (mask) {
+            // the lane's candidates in column order, values read back from
+            // its staging row (the loop runs once per candidate)
+#pragma unroll
+            for (int j = 0; j < 32; j += 4)
+              *reinterpret_cast<int4 *>(row + j) = make_int4(y[j], y[j + 1], y[j + 2], y[j + 3]);
+            do {
+              const int j = __ffs(mask) - 1;
+              mask &= mask - 1;
+              if (cnt < cap) list[cnt] = make_int2(qq - row[j], id0 + c2 + h + j);
+              ++cnt;
+            } while (mask);
+          }
+        }
       }
-      uint32_t tot = 0;
-      for (int w = 0; w < BF_THREADS / 32; ++w) tot += wcount[w];
-      run += tot;
-      __syncthreads();
+      tc_fence_before();
+      __syncwarp();
+      if (lane == 0) mbar_arrive1(&sm.accempty[ab]);
     }
-    if (tid == 0) {
-      for (uint32_t j = 0; j < run; ++j) {
-        const HeapNode nd = list[j];
-        if (heap[1].d <= nd.d) continue;
-        heap[1] = nd;
-        heap_push_down(heap, (int)k, 1);
+    if (valid) {
+      counts[(uint64_t)q * nseg + seg] = min(cnt, cap);
+      if (!ok || cnt > cap) mark[q] = 1u;
+    }
+  }
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(SQ_TMEM_COLS));
+  }
+}
+
+// Step 3.
+__global__ void __launch_bounds__(SQ_WARPS * 32, 4)
+    k_sq8_tail(const int8_t *__restrict__ codes, const int *__restrict__ ncc, uint64_t prefix, uint64_t npoints,
+               const int8_t *__restrict__ queries, uint32_t nq, uint32_t k, const HeapNode *__restrict__ heaps,
+               const int2 *__restrict__ cand, uint32_t cap, const uint32_t *__restrict__ counts, uint32_t nseg,
+               const uint32_t *__restrict__ mark, int *__restrict__ closest, float *__restrict__ dists, float alpha) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const uint32_t q = blockIdx.x * SQ_WARPS + warp;
+  if (q >= nq) return;  // warp-uniform; the kernel has no block barrier
+  HeapNode *heap = reinterpret_cast<HeapNode *>(smem_raw) + (size_t)warp * sq_region(k);
+  HeapNode *stage = heap + (sq_region(k) - SQ_SCAN);
+  for (uint32_t l = lane; l <= k; l += 32) heap[l] = heaps[(uint64_t)q * (k + 1) + l];
+  __syncwarp();
+  if (mark[q]) {
+    int4 qv[7];
+    int qq;
+    load_query(queries, q, qv, qq);
+    scan_codes(heap, stage, qv, qq, codes, ncc, prefix, npoints, k, lane);
+  } else {
+    const uint32_t below = (1u << lane) - 1u;
+    for (uint32_t s = 0; s < nseg; ++s) {
+      const uint32_t cnt = counts[(uint64_t)q * nseg + s];
+      const int2 *list = cand + ((uint64_t)q * nseg + s) * cap;
+      for (uint32_t j0 = 0; j0 < cnt; j0 += SQ_SCAN) {
+        int2 cd[SQ_SCAN / 32];
+#pragma unroll
+        for (int i = 0; i < SQ_SCAN / 32; ++i) {
+          const uint32_t j = j0 + 32 * i + lane;
+          cd[i] = j < cnt ? list[j] : make_int2(INT_MAX, 0);
+        }
+        const int root = heap[1].d;
+        int off = 0;
+#pragma unroll
+        for (int i = 0; i < SQ_SCAN / 32; ++i) {
+          const uint32_t m = __ballot_sync(0xffffffffu, cd[i].x < root);
+          if ((m >> lane) & 1u) {
+            HeapNode nd;
+            nd.d = cd[i].x;
+            nd.id = cd[i].y;
+            stage[off + __popc(m & below)] = nd;
+          }
+          off += __popc(m);
+        }
+        __syncwarp();
+        offer_list(heap, (int)k, stage, off, lane);
       }
     }
-    __syncthreads();
   }
-  // closest_points[k - l - 1] = data_[l + 1].id (bruteforce.h:262-264)
-  for (uint32_t l = tid; l < k; l += BF_THREADS) {
-    closest[(uint64_t)qi * k + (k - l - 1)] = heap[l + 1].id;
-    if (dists) dists[(uint64_t)qi * k + (k - l - 1)] = (float)heap[l + 1].d * alpha * alpha;
-  }
+  __syncwarp();
+  write_heap(heap, k, q, closest, dists, alpha, lane);
 }
 
 bool is_dev(const void *p) {
@@ -240,11 +586,51 @@ int sq8_encode_impl(const float *vecs, uint64_t n, float alpha, int8_t *codes, b
   return FKNN_OK;
 }
 
+// Device scratch of the slab brute force, kept between calls (it only
+// grows) and used by one call at a time.
+struct Sq8Scratch {
+  std::mutex mu;
+  void *p = nullptr;
+  size_t bytes = 0;
+};
+
+Sq8Scratch &sq8_scratch() {
+  static Sq8Scratch s;
+  return s;
+}
+
+size_t al256(size_t b) { return (b + 255) & ~(size_t)255; }
+
+// segments and list capacity for a pass of nqb queries over nct code tiles
+struct Sq8Pass {
+  uint32_t nqt, tps, nseg, cap;
+  size_t bytes;  // query tiles, norms, heaps, bounds, lists, counts, marks
+};
+
+Sq8Pass sq8_pass(uint32_t nqb, uint32_t nct, size_t k, int num_sms) {
+  Sq8Pass p{};
+  p.nqt = (nqb + TC_ROWS - 1) / TC_ROWS;
+  // about four screen CTAs per SM (two resident, two waves)
+  uint32_t nseg = std::max(1u, std::min(nct, (uint32_t)((4u * num_sms + p.nqt - 1) / p.nqt)));
+  p.tps = (nct + nseg - 1) / nseg;
+  p.nseg = (nct + p.tps - 1) / p.tps;
+  // a code of the screened part is a candidate iff it is below the k-th
+  // smallest of the prefix: about k / SQ_PREFIX of them; the lists hold twice
+  // that, and a query whose list fills up takes the exact scan
+  const double expect = (double)p.tps * TC_ROWS * (double)k / SQ_PREFIX;
+  p.cap = (uint32_t)std::min<double>((double)p.tps * TC_ROWS, ((uint32_t)(2.0 * expect) + 64 + 31) & ~31u);
+  p.bytes = al256((size_t)p.nqt * SQ_TILE) + al256((size_t)p.nqt * TC_ROWS * 4) +
+            al256((size_t)nqb * (k + 1) * sizeof(HeapNode)) + al256((size_t)nqb * 4) +
+            al256((size_t)nqb * p.nseg * p.cap * sizeof(int2)) + al256((size_t)nqb * p.nseg * 4) +
+            al256((size_t)nqb * 4) + 256;
+  return p;
+}
+
 int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char *codes_in, float alpha,
                 size_t nqueries, const int8_t *queries_in) {
   if (!closest || !codes_in || !queries_in || k == 0 || k > npoints || k > (size_t)BF_KMAX || nqueries == 0 ||
-      npoints >= (1ull << 31)) {
-    set_error("fknn_sq8_bruteforce: need 1 <= k <= npoints, k <= 2048, nqueries >= 1, npoints < 2^31");
+      npoints >= (1ull << 31) || nqueries >= (1ull << 31)) {
+    set_error("fknn_sq8_bruteforce: need 1 <= k <= npoints, k <= 2048, 1 <= nqueries < 2^31, npoints < 2^31");
     return FKNN_EINVAL;
   }
   int rc = ensure_device();
@@ -259,15 +645,88 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   if ((rc = stage_out(closest, nqueries * k * 4, si, (void **)&d_ids))) return rc;
   if (dists)
     if ((rc = stage_out(dists, nqueries * k * 4, sd, (void **)&d_d))) return rc;
-  const size_t smem = (k + 1 + BF_CHUNK) * sizeof(HeapNode);
-  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_bruteforce, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_sq8_bruteforce<<<(unsigned)nqueries, BF_THREADS, smem, st>>>(d_codes, npoints, d_q, (uint32_t)k, d_ids, d_d,
-                                                                 alpha);
-  g_launches += 1;
-  FKNN_CUDA(cudaGetLastError());
+
+  int dev = 0, num_sms = 148;
+  FKNN_CUDA(cudaGetDevice(&dev));
+  FKNN_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  const uint32_t nq = (uint32_t)nqueries, K = (uint32_t)k;
+  const bool screened = npoints > SQ_PREFIX;
+  const uint64_t prefix = screened ? SQ_PREFIX : npoints;
+  const uint32_t nct_all = (uint32_t)((npoints + TC_ROWS - 1) / TC_ROWS);
+  const uint32_t nct = screened ? nct_all - SQ_PREFIX / TC_ROWS : 0;
+  const uint32_t qbatch = std::min(nq, SQ_QBATCH);
+  const uint32_t qlast = nq - (nq - 1) / qbatch * qbatch;
+  const Sq8Pass pa = sq8_pass(qbatch, std::max(nct, 1u), k, num_sms);
+  const Sq8Pass pb = sq8_pass(qlast, std::max(nct, 1u), k, num_sms);
+  const size_t codes_bytes = al256((size_t)nct_all * SQ_TILE) + al256((size_t)nct_all * TC_ROWS * 4);
+  const size_t need = codes_bytes + std::max(pa.bytes, pb.bytes) + 256;
+
+  Sq8Scratch &scr = sq8_scratch();
+  std::lock_guard<std::mutex> lock(scr.mu);
+  if (scr.bytes < need) {
+    if (scr.p) cudaFree(scr.p);
+    scr.p = nullptr;
+    scr.bytes = 0;
+    FKNN_CUDA(cudaMalloc(&scr.p, need));
+    scr.bytes = need;
+  }
+  unsigned char *base = static_cast<unsigned char *>(scr.p);
+  unsigned char *ctiles = base;
+  int *cncc = reinterpret_cast<int *>(base + al256((size_t)nct_all * SQ_TILE));
+  unsigned char *pass_base = base + codes_bytes;
+  int *d_err = reinterpret_cast<int *>(base + codes_bytes + std::max(pa.bytes, pb.bytes));
+
+  const size_t rsmem = (size_t)SQ_WARPS * sq_region(K) * sizeof(HeapNode);
+  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_prefix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
+  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(SqScreenSmem)));
+  FKNN_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
+  // |c|^2 of every code (the replay kernels use it too) and the tiles
+  k_sq8_tiles<<<nct_all, 256, 0, st>>>(d_codes, npoints, 0, ctiles, cncc);
+  g_launches += 2;
+  for (uint32_t q0 = 0; q0 < nq; q0 += qbatch) {
+    const uint32_t nqb = std::min(qbatch, nq - q0);
+    const Sq8Pass ps = sq8_pass(nqb, std::max(nct, 1u), k, num_sms);
+    size_t off = 0;
+    auto take = [&](size_t b) {
+      unsigned char *p = pass_base + off;
+      off += al256(b);
+      return p;
+    };
+    unsigned char *qtiles = take((size_t)ps.nqt * SQ_TILE);
+    int *qncc = reinterpret_cast<int *>(take((size_t)ps.nqt * TC_ROWS * 4));
+    HeapNode *heaps = reinterpret_cast<HeapNode *>(take((size_t)nqb * (k + 1) * sizeof(HeapNode)));
+    int *T = reinterpret_cast<int *>(take((size_t)nqb * 4));
+    int2 *cand = reinterpret_cast<int2 *>(take((size_t)nqb * ps.nseg * ps.cap * sizeof(int2)));
+    uint32_t *counts = reinterpret_cast<uint32_t *>(take((size_t)nqb * ps.nseg * 4));
+    uint32_t *mark = reinterpret_cast<uint32_t *>(take((size_t)nqb * 4));
+    const int8_t *qs = d_q + (uint64_t)q0 * SQ8_CODE;
+    int *ids = d_ids + (uint64_t)q0 * k;
+    float *dd = d_d ? d_d + (uint64_t)q0 * k : nullptr;
+    const unsigned rblocks = (nqb + SQ_WARPS - 1) / SQ_WARPS;
+    k_sq8_prefix<<<rblocks, SQ_WARPS * 32, rsmem, st>>>(d_codes, cncc, prefix, qs, nqb, K, screened ? 0 : 1, heaps,
+                                                        T, ids, dd, alpha);
+    g_launches += 1;
+    if (screened) {
+      FKNN_CUDA(cudaMemsetAsync(mark, 0, (size_t)nqb * 4, st));
+      k_sq8_tiles<<<ps.nqt, 256, 0, st>>>(qs, nqb, 0, qtiles, qncc);
+      k_sq8_screen<<<dim3(ps.nqt, ps.nseg), SQ_THREADS, sizeof(SqScreenSmem), st>>>(
+          qtiles, qncc, nqb, ctiles + (size_t)(SQ_PREFIX / TC_ROWS) * SQ_TILE, cncc + SQ_PREFIX, nct, ps.tps, ps.nseg,
+          SQ_PREFIX, T, cand, ps.cap, counts, mark, d_err);
+      k_sq8_tail<<<rblocks, SQ_WARPS * 32, rsmem, st>>>(d_codes, cncc, SQ_PREFIX, npoints, qs, nqb, K, heaps, cand,
+                                                        ps.cap, counts, ps.nseg, mark, ids, dd, alpha);
+      g_launches += 3;
+    }
+    FKNN_CUDA(cudaGetLastError());
+  }
   if (d_ids != closest) FKNN_CUDA(cudaMemcpyAsync(closest, d_ids, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && d_d != dists) FKNN_CUDA(cudaMemcpyAsync(dists, d_d, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
+  int err = 0;
+  FKNN_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
+  if (err & ERR_WAIT_TIMEOUT)
+    set_error("fknn_sq8_bruteforce: a bounded device wait gave up; affected queries were answered by the exact scan");
   return FKNN_OK;
 }
 

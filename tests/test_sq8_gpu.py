@@ -62,6 +62,25 @@ def test_bruteforce_matches_oracle(npoints, k):
         np.testing.assert_array_equal(d[i], od)
 
 
+@pytest.mark.parametrize("nq,k", [(9, 2048), (17, 140), (2, 7)])
+def test_bruteforce_batched_matches_single(nq, k):
+    """The batched kernel (eight queries per block, short last block) returns
+    what one-query calls return, at the largest k too."""
+    rng = np.random.default_rng(nq * 1000 + k)
+    base = rng.standard_normal((4000, 100), dtype=np.float32)
+    vecs = np.repeat(base, 2, axis=0)
+    alpha, codes = oracle.sq8_sym_train(vecs)
+    qv = oracle.sq8_sym_encode(rng.standard_normal((nq, 100), dtype=np.float32), alpha)
+    out = np.empty((nq, k), dtype=np.int32)
+    fknn.bruteforce(100, k, out, codes.shape[0], codes, alpha, nq, qv)
+    for i in range(nq):
+        one = np.empty(k, dtype=np.int32)
+        fknn.bruteforce(100, k, one, codes.shape[0], codes, alpha, 1, np.ascontiguousarray(qv[i]))
+        np.testing.assert_array_equal(out[i], one)
+        if i % 4 == 0:
+            np.testing.assert_array_equal(out[i], oracle.sq8_bruteforce(k, codes, alpha, qv[i]))
+
+
 def test_bruteforce_rejects_bad_k():
     codes = np.zeros((10, 112), np.int8)
     out = np.empty(11, np.int32)
