@@ -129,18 +129,13 @@ __device__ __forceinline__ void heap_offer(HeapNode *h, int cnt, HeapNode nd) {
   while ((x << 1) <= cnt) {
     const int t0 = x << 1;
     const int4 pr = *reinterpret_cast<const int4 *>(h + t0);
-    int t = t0;
+    const bool r = t0 < cnt && pr.z > pr.x;
     HeapNode c;
-    c.d = pr.x;
-    c.id = pr.y;
-    if (t0 + 1 <= cnt && pr.z > pr.x) {
-      t = t0 + 1;
-      c.d = pr.z;
-      c.id = pr.w;
-    }
+    c.d = r ? pr.z : pr.x;
+    c.id = r ? pr.w : pr.y;
     if (c.d <= nd.d) break;
     h[x] = c;
-    x = t;
+    x = t0 + (r ? 1 : 0);
   }
   h[x] = nd;
 }
@@ -222,29 +217,56 @@ __device__ __forceinline__ void write_heap(const HeapNode *heap, uint32_t k, uin
   }
 }
 
+// The screen's accumulator carries most of -|c|^2/2: bytes 112..127 of a
+// row (zero padding in every SQ8 code, so the dot product is unchanged) hold
+// base-127 digits of f = min(ceil(|c|^2 / 2), SQ_FOLD_MAX) on the code side --
+// fifteen digits of weight 127 and one of weight 1 -- and the multipliers
+// -127 / -1 on the query side, so the MMA returns z = q.c - f.
+constexpr int SQ_FOLD_MAX = 127 * (15 * 127) + 126;
+
+__host__ __device__ __forceinline__ int sq_fold(int cc) { return min((cc + 1) >> 1, SQ_FOLD_MAX); }
+
 // Rows [row0, row0 + 128 * ntiles) of n rows of 112 bytes as 128-row
-// core-matrix tiles of 128 bytes per row (bytes 112..127 and rows past n
-// zero), and ncc[r] = -|row r|^2 (SQ_NCC_PAD past n).  One block per tile.
+// core-matrix tiles of 128 bytes per row (rows past n zero), bytes 112..127
+// the fold digits (side 0, codes) or multipliers (side 1, queries), and
+// ncc[r] = -|row r|^2 (SQ_NCC_PAD past n).  One block per tile.
 __global__ void __launch_bounds__(256) k_sq8_tiles(const int8_t *__restrict__ rows, uint64_t n, uint64_t row0,
-                                                   unsigned char *__restrict__ tiles, int *__restrict__ ncc) {
+                                                   int side, unsigned char *__restrict__ tiles,
+                                                   int *__restrict__ ncc) {
   const uint64_t t = blockIdx.x;
   unsigned char *o = tiles + t * SQ_TILE;
   for (uint32_t c = threadIdx.x; c < TC_ROWS * 8; c += blockDim.x) {
     const uint32_t r = c >> 3, kc = c & 7;
     const uint64_t p = row0 + t * TC_ROWS + r;
     int4 v = make_int4(0, 0, 0, 0);
-    if (kc < 7 && p < n) v = __ldg(reinterpret_cast<const int4 *>(rows + p * SQ8_CODE) + kc);
-    *reinterpret_cast<int4 *>(o + cm_byte(r, kc * 16)) = v;
-  }
-  for (uint32_t r = threadIdx.x; r < (uint32_t)TC_ROWS; r += blockDim.x) {
-    const uint64_t p = row0 + t * TC_ROWS + r;
-    int v = SQ_NCC_PAD;
     if (p < n) {
-      int4 c[7];
-      load_code(rows, p, n, c);
-      v = -dot112(c, c);
+      if (kc < 7) {
+        v = __ldg(reinterpret_cast<const int4 *>(rows + p * SQ8_CODE) + kc);
+      } else {
+        int4 cw[7];
+        load_code(rows, p, n, cw);
+        const int cc = dot112(cw, cw);
+        ncc[t * TC_ROWS + r] = -cc;
+        int8_t b[16];
+        if (side == 0) {
+          const int f = sq_fold(cc);
+          int e = f / 127;
+          for (int i = 0; i < 15; ++i) {
+            const int di = e > 127 ? 127 : e;
+            b[i] = (int8_t)di;
+            e -= di;
+          }
+          b[15] = (int8_t)(f % 127);
+        } else {
+          for (int i = 0; i < 15; ++i) b[i] = (int8_t)-127;
+          b[15] = (int8_t)-1;
+        }
+        memcpy(&v, b, 16);
+      }
+    } else if (kc == 7) {
+      ncc[t * TC_ROWS + r] = SQ_NCC_PAD;
     }
-    ncc[t * TC_ROWS + r] = v;
+    *reinterpret_cast<int4 *>(o + cm_byte(r, kc * 16)) = v;
   }
 }
 
@@ -299,8 +321,8 @@ __device__ __forceinline__ void umma_i8(uint32_t tmem_d, uint64_t da, uint64_t d
 __global__ void __launch_bounds__(SQ_THREADS, 2)
     k_sq8_screen(const unsigned char *__restrict__ qtiles, const int *__restrict__ qncc, uint32_t nq,
                  const unsigned char *__restrict__ ctiles, const int *__restrict__ cncc, uint32_t nct, uint32_t tps,
-                 uint32_t nseg, uint32_t row0, const int *__restrict__ T, int2 *__restrict__ cand, uint32_t cap,
-                 uint32_t *__restrict__ counts, uint32_t *__restrict__ mark, int *err) {
+                 uint32_t nseg, uint32_t row0, uint64_t npoints, const int *__restrict__ T, int2 *__restrict__ cand,
+                 uint32_t cap, uint32_t *__restrict__ counts, uint32_t *__restrict__ mark, int *err) {
   extern __shared__ __align__(1024) unsigned char screen_smem[];
   SqScreenSmem &sm = *reinterpret_cast<SqScreenSmem *>(screen_smem);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -379,9 +401,12 @@ __global__ void __launch_bounds__(SQ_THREADS, 2)
     const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
     const uint32_t q = qt * TC_ROWS + wg * 32 + lane;
     const bool valid = q < nq;
-    // candidate iff d = qq - y < T with y = 2 q.c - |c|^2, i.e. y > qq - T
+    // The accumulator is z = q.c - f with f = sq_fold(|c|^2) <= (|c|^2 + 1) / 2,
+    // so d = qq + |c|^2 - 2 q.c < T implies 2 z > qq - T - 1: the test
+    // z > floor((qq - T - 1) / 2) keeps every code that can enter the heap
+    // (and a few more), and d = qq + cc - 2 (z + f) is exact.
     const int qq = valid ? -qncc[q] : 0;
-    const int thr = valid ? qq - T[q] : INT_MAX;
+    const int thr = valid ? ((qq - T[q] - 1) >> 1) : INT_MAX;
     int2 *list = cand + ((uint64_t)(valid ? q : 0) * nseg + seg) * cap;
     int *row = &sm.stage[wg][lane * SQ_STAGE_ROW];
     uint32_t cnt = 0;
@@ -396,36 +421,33 @@ __global__ void __launch_bounds__(SQ_THREADS, 2)
       const uint32_t tile = t0 + sub;
       const int *nc = cncc + (uint64_t)tile * TC_ROWS;
       const int id0 = (int)(row0 + tile * TC_ROWS);
+      const int ncols = (int)min((uint64_t)TC_ROWS, npoints - (uint64_t)id0);  // the slab's last tile is short
 #pragma unroll 1
       for (int c2 = 0; c2 < TC_ROWS; c2 += 64) {
         float v[64];
         tmem_ld64(tmem + ((uint32_t)(wg * 32) << 16) + ab * TC_ROWS + c2, v);
 #pragma unroll
         for (int h = 0; h < 64; h += 32) {
-          // y for 32 columns and the candidate bits, four independent chains
-          int y[32];
+          // candidate bits of 32 columns, four independent chains
           uint32_t mk[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
-          for (int j = 0; j < 32; j += 4) {
-            const int4 n4 = __ldg(reinterpret_cast<const int4 *>(nc + c2 + h + j));
-            y[j] = 2 * __float_as_int(v[h + j]) + n4.x;
-            y[j + 1] = 2 * __float_as_int(v[h + j + 1]) + n4.y;
-            y[j + 2] = 2 * __float_as_int(v[h + j + 2]) + n4.z;
-            y[j + 3] = 2 * __float_as_int(v[h + j + 3]) + n4.w;
-#pragma unroll
-            for (int g = 0; g < 4; ++g) mk[g] |= (y[j + g] > thr ? 1u : 0u) << (j + g);
-          }
+          for (int j = 0; j < 32; ++j) mk[j & 3] |= (__float_as_int(v[h + j]) > thr ? 1u : 0u) << j;
           uint32_t mask = (mk[0] | mk[1]) | (mk[2] | mk[3]);
+          const int lim = ncols - (c2 + h);
+          if (lim < 32) mask &= lim > 0 ? (1u << lim) - 1u : 0u;
           if (mask) {
-            // the lane's candidates in column order, values read back from
-            // its staging row (the loop runs once per candidate)
+            // the lane's candidates in column order, z read back from its
+            // staging row (the loop runs once per candidate)
 #pragma unroll
             for (int j = 0; j < 32; j += 4)
-              *reinterpret_cast<int4 *>(row + j) = make_int4(y[j], y[j + 1], y[j + 2], y[j + 3]);
+              *reinterpret_cast<int4 *>(row + j) =
+                  make_int4(__float_as_int(v[h + j]), __float_as_int(v[h + j + 1]), __float_as_int(v[h + j + 2]),
+                            __float_as_int(v[h + j + 3]));
             do {
               const int j = __ffs(mask) - 1;
               mask &= mask - 1;
-              if (cnt < cap) list[cnt] = make_int2(qq - row[j], id0 + c2 + h + j);
+              const int cc = -__ldg(nc + c2 + h + j);
+              if (cnt < cap) list[cnt] = make_int2(qq + cc - 2 * (row[j] + sq_fold(cc)), id0 + c2 + h + j);
               ++cnt;
             } while (mask);
           }
@@ -683,7 +705,7 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
                                  (int)sizeof(SqScreenSmem)));
   FKNN_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   // |c|^2 of every code (the replay kernels use it too) and the tiles
-  k_sq8_tiles<<<nct_all, 256, 0, st>>>(d_codes, npoints, 0, ctiles, cncc);
+  k_sq8_tiles<<<nct_all, 256, 0, st>>>(d_codes, npoints, 0, 0, ctiles, cncc);
   g_launches += 2;
   for (uint32_t q0 = 0; q0 < nq; q0 += qbatch) {
     const uint32_t nqb = std::min(qbatch, nq - q0);
@@ -710,10 +732,10 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
     g_launches += 1;
     if (screened) {
       FKNN_CUDA(cudaMemsetAsync(mark, 0, (size_t)nqb * 4, st));
-      k_sq8_tiles<<<ps.nqt, 256, 0, st>>>(qs, nqb, 0, qtiles, qncc);
+      k_sq8_tiles<<<ps.nqt, 256, 0, st>>>(qs, nqb, 0, 1, qtiles, qncc);
       k_sq8_screen<<<dim3(ps.nqt, ps.nseg), SQ_THREADS, sizeof(SqScreenSmem), st>>>(
           qtiles, qncc, nqb, ctiles + (size_t)(SQ_PREFIX / TC_ROWS) * SQ_TILE, cncc + SQ_PREFIX, nct, ps.tps, ps.nseg,
-          SQ_PREFIX, T, cand, ps.cap, counts, mark, d_err);
+          SQ_PREFIX, npoints, T, cand, ps.cap, counts, mark, d_err);
       k_sq8_tail<<<rblocks, SQ_WARPS * 32, rsmem, st>>>(d_codes, cncc, SQ_PREFIX, npoints, qs, nqb, K, heaps, cand,
                                                         ps.cap, counts, ps.nseg, mark, ids, dd, alpha);
       g_launches += 3;

@@ -81,6 +81,38 @@ def test_bruteforce_batched_matches_single(nq, k):
             np.testing.assert_array_equal(out[i], oracle.sq8_bruteforce(k, codes, alpha, qv[i]))
 
 
+@pytest.mark.parametrize("npoints,nq,k", [(20000, 9, 2048), (40000, 130, 140)])
+def test_bruteforce_screened_batch(npoints, nq, k):
+    """Slabs past the exactly replayed prefix go through the int8 tensor-core
+    screen; the batch (a short last query tile included) must give the
+    oracle's heap arrays at the largest k and at the reference's K'."""
+    rng = np.random.default_rng(npoints + nq)
+    base = rng.standard_normal((npoints // 2, 100), dtype=np.float32)
+    vecs = np.repeat(base, 2, axis=0)  # many equal distances
+    alpha, codes = oracle.sq8_sym_train(vecs)
+    qv = oracle.sq8_sym_encode(rng.standard_normal((nq, 100), dtype=np.float32), alpha)
+    out = np.empty((nq, k), dtype=np.int32)
+    d = np.empty((nq, k), dtype=np.float32)
+    fknn.bruteforce_subgraph(100, k, out, d, npoints, codes, alpha, nq, qv)
+    for i in list(range(0, nq, max(1, nq // 6))) + [nq - 1]:
+        oi, od = oracle.sq8_bruteforce(k, codes, alpha, qv[i], with_dists=True)
+        np.testing.assert_array_equal(out[i], oi)
+        np.testing.assert_array_equal(d[i], od)
+
+
+def test_bruteforce_full_width_codes():
+    """The distance runs over all 112 code bytes (L2SqrSQ8_sym with d = 112),
+    padding bytes included, on the prefix and the screened part alike."""
+    rng = np.random.default_rng(7)
+    npoints, nq, k = 30000, 5, 140
+    codes = rng.integers(-127, 128, size=(npoints, 112), dtype=np.int8)
+    qv = rng.integers(-127, 128, size=(nq, 112), dtype=np.int8)
+    out = np.empty((nq, k), dtype=np.int32)
+    fknn.bruteforce(100, k, out, npoints, codes, 1.0, nq, qv)
+    for i in range(nq):
+        np.testing.assert_array_equal(out[i], oracle.sq8_bruteforce(k, codes, 1.0, qv[i]))
+
+
 def test_bruteforce_rejects_bad_k():
     codes = np.zeros((10, 112), np.int8)
     out = np.empty(11, np.int32)
