@@ -72,6 +72,9 @@ def parse():
     ap.add_argument("--sq8", action="store_true",
                     help="SQ8 slab brute force instead of the headline (bruteforce.h:244 with K'=140): codes/s and "
                          "GB/s over a slab of 4.5 %% of N=1e7 codes, batched queries")
+    ap.add_argument("--sq8-callers", type=int, default=0,
+                    help="with --sq8: this many host threads each calling with one query at a time, as the "
+                         "reference's OpenMP workers do (hybrid_graph.cpp:211)")
     ap.add_argument("--graph", action="store_true",
                     help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
                          "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
@@ -559,19 +562,41 @@ def run_sq8(args):
     def call():
         _lib.check(lib.fknn_sq8_bruteforce_subgraph(100, k, ids.data_ptr(), dd.data_ptr(), npoints, codes.data_ptr(),
                                                     ctypes.c_float(quant.alpha), nq, qc.data_ptr()))
-    for _ in range(args.warmup):
-        call()
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        call()
-    torch.cuda.synchronize()
+    if args.sq8_callers:
+        # T host threads, each answering its share of the queries one call
+        # per query; wall time over all of them (each call is synchronous)
+        import concurrent.futures as cf
+        nthreads = args.sq8_callers
+        qrows = [qc[i:i + 1] for i in range(nq)]
+
+        def worker(t):
+            for i in range(t, nq, nthreads):
+                _lib.check(lib.fknn_sq8_bruteforce_subgraph(100, k, ids[i].data_ptr(), dd[i].data_ptr(), npoints,
+                                                            codes.data_ptr(), ctypes.c_float(quant.alpha), 1,
+                                                            qrows[i].data_ptr()))
+        with cf.ThreadPoolExecutor(nthreads) as ex:
+            for _ in range(args.warmup):
+                list(ex.map(worker, range(nthreads)))
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            for _ in range(args.steps):
+                list(ex.map(worker, range(nthreads)))
+            torch.cuda.synchronize()
+    else:
+        for _ in range(args.warmup):
+            call()
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            call()
+        torch.cuda.synchronize()
     sec = (time.perf_counter() - t0) / args.steps
     pairs = nq * npoints
     line = {"mode": "sq8", "metric": "SQ8 slab brute force, codes scanned per second",
             "value": pairs / sec, "unit": "codes/s", "gbs_algorithmic": pairs * 112 / sec / 1e9,
             "ms_per_call": sec * 1e3, "queries_per_s": nq / sec,
-            "config": {"slab_codes": npoints, "queries_per_call": nq, "k": k, "code_bytes": 112}}
+            "config": {"slab_codes": npoints, "queries_per_call": 1 if args.sq8_callers else nq,
+                       "queries_per_step": nq, "host_threads": args.sq8_callers or 1, "k": k, "code_bytes": 112}}
     # The reference's own bruteforce() (compiled from its sources) on the
     # host cores, one query per call as hybrid_graph.cpp:211 calls it, over a
     # sample of the same queries; its heap-array ids must equal ours.

@@ -7,7 +7,6 @@
 // above k_sq8_prefix).  Every distance is an exact int32 L2SqrSQ8_sym value:
 // |q-c|^2 = |q|^2 + |c|^2 - 2 q.c, from dp4a or from the int8 tensor cores.
 #include <climits>
-#include <mutex>
 
 #include "tc_util.cuh"
 
@@ -608,16 +607,33 @@ int sq8_encode_impl(const float *vecs, uint64_t n, float alpha, int8_t *codes, b
   return FKNN_OK;
 }
 
-// Device scratch of the slab brute force, kept between calls (it only
-// grows) and used by one call at a time.
+// Device scratch of the slab brute force: one per calling host thread, with
+// its own non-blocking stream, kept between calls (it only grows).  The
+// reference calls bruteforce() from concurrent OpenMP workers
+// (hybrid_graph.cpp:168,380); with a scratch and a stream each, their calls
+// run side by side on the GPU, and after the first call of a thread at a
+// given size none of them allocates (cudaFree would wait for the device).
 struct Sq8Scratch {
-  std::mutex mu;
   void *p = nullptr;
   size_t bytes = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev = nullptr;  // orders the call after the legacy default stream
+  int device = -1;
+  void release() {
+    if (p) cudaFree(p);
+    if (ev) cudaEventDestroy(ev);
+    if (st) cudaStreamDestroy(st);
+    p = nullptr;
+    ev = nullptr;
+    st = nullptr;
+    bytes = 0;
+    device = -1;
+  }
+  ~Sq8Scratch() { release(); }
 };
 
 Sq8Scratch &sq8_scratch() {
-  static Sq8Scratch s;
+  thread_local Sq8Scratch s;
   return s;
 }
 
@@ -657,17 +673,6 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   }
   int rc = ensure_device();
   if (rc) return rc;
-  cudaStream_t st = 0;
-  Scoped sc, sq, si, sd;
-  const int8_t *d_codes, *d_q;
-  int *d_ids;
-  float *d_d = nullptr;
-  if ((rc = stage_in(codes_in, npoints * SQ8_CODE, sc, (const void **)&d_codes, st))) return rc;
-  if ((rc = stage_in(queries_in, nqueries * SQ8_CODE, sq, (const void **)&d_q, st))) return rc;
-  if ((rc = stage_out(closest, nqueries * k * 4, si, (void **)&d_ids))) return rc;
-  if (dists)
-    if ((rc = stage_out(dists, nqueries * k * 4, sd, (void **)&d_d))) return rc;
-
   int dev = 0, num_sms = 148;
   FKNN_CUDA(cudaGetDevice(&dev));
   FKNN_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
@@ -680,11 +685,27 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   const uint32_t qlast = nq - (nq - 1) / qbatch * qbatch;
   const Sq8Pass pa = sq8_pass(qbatch, std::max(nct, 1u), k, num_sms);
   const Sq8Pass pb = sq8_pass(qlast, std::max(nct, 1u), k, num_sms);
+
+  // inputs already on the device (16-byte aligned) are used in place, the
+  // rest staged through the scratch, as are outputs that live on the host
+  const bool codes_dev = is_dev(codes_in) && ((uintptr_t)codes_in & 15) == 0;
+  const bool q_dev = is_dev(queries_in) && ((uintptr_t)queries_in & 15) == 0;
+  const bool ids_dev = is_dev(closest);
+  const bool d_dev = dists && is_dev(dists);
+  const size_t b_codes = codes_dev ? 0 : al256(npoints * SQ8_CODE);
+  const size_t b_q = q_dev ? 0 : al256(nqueries * SQ8_CODE);
+  const size_t b_ids = ids_dev ? 0 : al256(nqueries * k * 4);
+  const size_t b_d = (!dists || d_dev) ? 0 : al256(nqueries * k * 4);
   const size_t codes_bytes = al256((size_t)nct_all * SQ_TILE) + al256((size_t)nct_all * TC_ROWS * 4);
-  const size_t need = codes_bytes + std::max(pa.bytes, pb.bytes) + 256;
+  const size_t need = b_codes + b_q + b_ids + b_d + codes_bytes + std::max(pa.bytes, pb.bytes) + 256;
 
   Sq8Scratch &scr = sq8_scratch();
-  std::lock_guard<std::mutex> lock(scr.mu);
+  if (scr.device != dev) {
+    scr.release();
+    FKNN_CUDA(cudaStreamCreateWithFlags(&scr.st, cudaStreamNonBlocking));
+    FKNN_CUDA(cudaEventCreateWithFlags(&scr.ev, cudaEventDisableTiming));
+    scr.device = dev;
+  }
   if (scr.bytes < need) {
     if (scr.p) cudaFree(scr.p);
     scr.p = nullptr;
@@ -692,7 +713,24 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
     FKNN_CUDA(cudaMalloc(&scr.p, need));
     scr.bytes = need;
   }
+  const cudaStream_t st = scr.st;
+  // device inputs are read in place: whatever the legacy default stream (and
+  // the blocking streams it orders) has queued so far comes first
+  FKNN_CUDA(cudaEventRecord(scr.ev, 0));
+  FKNN_CUDA(cudaStreamWaitEvent(st, scr.ev, 0));
   unsigned char *base = static_cast<unsigned char *>(scr.p);
+  const int8_t *d_codes = codes_dev ? reinterpret_cast<const int8_t *>(codes_in) : reinterpret_cast<int8_t *>(base);
+  base += b_codes;
+  const int8_t *d_q = q_dev ? queries_in : reinterpret_cast<int8_t *>(base);
+  base += b_q;
+  int *d_ids = ids_dev ? closest : reinterpret_cast<int *>(base);
+  base += b_ids;
+  float *d_d = !dists ? nullptr : d_dev ? dists : reinterpret_cast<float *>(base);
+  base += b_d;
+  if (!codes_dev)
+    FKNN_CUDA(cudaMemcpyAsync(const_cast<int8_t *>(d_codes), codes_in, npoints * SQ8_CODE, cudaMemcpyDefault, st));
+  if (!q_dev)
+    FKNN_CUDA(cudaMemcpyAsync(const_cast<int8_t *>(d_q), queries_in, nqueries * SQ8_CODE, cudaMemcpyDefault, st));
   unsigned char *ctiles = base;
   int *cncc = reinterpret_cast<int *>(base + al256((size_t)nct_all * SQ_TILE));
   unsigned char *pass_base = base + codes_bytes;
@@ -742,8 +780,8 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
     }
     FKNN_CUDA(cudaGetLastError());
   }
-  if (d_ids != closest) FKNN_CUDA(cudaMemcpyAsync(closest, d_ids, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
-  if (dists && d_d != dists) FKNN_CUDA(cudaMemcpyAsync(dists, d_d, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
+  if (!ids_dev) FKNN_CUDA(cudaMemcpyAsync(closest, d_ids, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
+  if (dists && !d_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_d, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
   int err = 0;
   FKNN_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));

@@ -113,6 +113,39 @@ def test_bruteforce_full_width_codes():
         np.testing.assert_array_equal(out[i], oracle.sq8_bruteforce(k, codes, 1.0, qv[i]))
 
 
+def test_bruteforce_concurrent_callers():
+    """The reference calls bruteforce() one query at a time from concurrent
+    OpenMP workers (hybrid_graph.cpp:168,380).  Host threads calling at once,
+    each on its own slab (prefix-only and screened sizes), get what the same
+    calls return one after another."""
+    import concurrent.futures as cf
+    rng = np.random.default_rng(11)
+    sizes = [3000, 9000, 12000, 20000, 5000, 16000]
+    jobs = []
+    for n in sizes:
+        vecs = np.repeat(rng.standard_normal((n // 2, 100), dtype=np.float32), 2, axis=0)
+        alpha, codes = oracle.sq8_sym_train(vecs)
+        qv = oracle.sq8_sym_encode(rng.standard_normal((6, 100), dtype=np.float32), alpha)
+        jobs.append((n, codes, alpha, qv))
+    k = 140
+
+    def run(job):
+        n, codes, alpha, qv = job
+        out = np.empty((qv.shape[0], k), dtype=np.int32)
+        for i in range(qv.shape[0]):
+            fknn.bruteforce(100, k, out[i], n, codes, alpha, 1, np.ascontiguousarray(qv[i]))
+        return out
+
+    serial = [run(j) for j in jobs]
+    for _ in range(2):
+        with cf.ThreadPoolExecutor(len(jobs)) as ex:
+            par = list(ex.map(run, jobs))
+        for a, b in zip(serial, par):
+            np.testing.assert_array_equal(a, b)
+    n, codes, alpha, qv = jobs[3]
+    np.testing.assert_array_equal(serial[3][0], oracle.sq8_bruteforce(k, codes, alpha, qv[0]))
+
+
 def test_bruteforce_rejects_bad_k():
     codes = np.zeros((10, 112), np.int8)
     out = np.empty(11, np.int32)
