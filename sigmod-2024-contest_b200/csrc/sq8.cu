@@ -780,6 +780,10 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
     }
     FKNN_CUDA(cudaGetLastError());
   }
+  // the kernels finish before any copy to (pageable) host memory is queued,
+  // so those copies do not wait on the GPU inside the driver's copy path,
+  // where concurrent callers' copies would queue behind them
+  FKNN_CUDA(cudaStreamSynchronize(st));
   if (!ids_dev) FKNN_CUDA(cudaMemcpyAsync(closest, d_ids, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
   if (dists && !d_dev) FKNN_CUDA(cudaMemcpyAsync(dists, d_d, nqueries * k * 4, cudaMemcpyDeviceToHost, st));
   int err = 0;
