@@ -182,7 +182,11 @@ int fknn_sq8_sym_encode(const float *vecs, uint64_t n, float alpha, int8_t *code
  * slab of npoints x 112 int8 codes, queries_in nqueries x 112 int8.  Unlike
  * the reference, nqueries is honoured: closest_points is nqueries x k, each
  * row in the reference's heap-array order.  dim and alpha are ignored, as in
- * the reference.  Requires 1 <= k <= npoints. */
+ * the reference.  Requires 1 <= k <= 2048 and k <= npoints < 2^31.  Pointers
+ * may be host or device memory (device codes and queries 16-byte aligned are
+ * read in place, after the work queued on the legacy default stream).  The
+ * call is synchronous and reentrant: each calling host thread has its own
+ * device scratch and stream, kept between calls. */
 int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoints, const char *codes_in,
                         float alpha, size_t nqueries, const int8_t *queries_in);
 
