@@ -619,6 +619,7 @@ struct Sq8Scratch {
   cudaStream_t st = nullptr;
   cudaEvent_t ev = nullptr;  // orders the call after the legacy default stream
   int device = -1;
+  int num_sms = 0;
   void release() {
     if (p) cudaFree(p);
     if (ev) cudaEventDestroy(ev);
@@ -673,9 +674,24 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   }
   int rc = ensure_device();
   if (rc) return rc;
-  int dev = 0, num_sms = 148;
+  int dev = 0;
   FKNN_CUDA(cudaGetDevice(&dev));
-  FKNN_CUDA(cudaDeviceGetAttribute(&num_sms, cudaDevAttrMultiProcessorCount, dev));
+  Sq8Scratch &scr = sq8_scratch();
+  if (scr.device != dev) {
+    // once per thread and device: stream, event, SM count, and the kernels'
+    // dynamic shared-memory limits at their largest (k = BF_KMAX)
+    scr.release();
+    FKNN_CUDA(cudaStreamCreateWithFlags(&scr.st, cudaStreamNonBlocking));
+    FKNN_CUDA(cudaEventCreateWithFlags(&scr.ev, cudaEventDisableTiming));
+    FKNN_CUDA(cudaDeviceGetAttribute(&scr.num_sms, cudaDevAttrMultiProcessorCount, dev));
+    const int rmax = (int)((size_t)SQ_WARPS * sq_region(BF_KMAX) * sizeof(HeapNode));
+    FKNN_CUDA(cudaFuncSetAttribute(k_sq8_prefix, cudaFuncAttributeMaxDynamicSharedMemorySize, rmax));
+    FKNN_CUDA(cudaFuncSetAttribute(k_sq8_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, rmax));
+    FKNN_CUDA(cudaFuncSetAttribute(k_sq8_screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                   (int)sizeof(SqScreenSmem)));
+    scr.device = dev;
+  }
+  const int num_sms = scr.num_sms;
   const uint32_t nq = (uint32_t)nqueries, K = (uint32_t)k;
   const bool screened = npoints > SQ_PREFIX;
   const uint64_t prefix = screened ? SQ_PREFIX : npoints;
@@ -699,13 +715,6 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   const size_t codes_bytes = al256((size_t)nct_all * SQ_TILE) + al256((size_t)nct_all * TC_ROWS * 4);
   const size_t need = b_codes + b_q + b_ids + b_d + codes_bytes + std::max(pa.bytes, pb.bytes) + 256;
 
-  Sq8Scratch &scr = sq8_scratch();
-  if (scr.device != dev) {
-    scr.release();
-    FKNN_CUDA(cudaStreamCreateWithFlags(&scr.st, cudaStreamNonBlocking));
-    FKNN_CUDA(cudaEventCreateWithFlags(&scr.ev, cudaEventDisableTiming));
-    scr.device = dev;
-  }
   if (scr.bytes < need) {
     if (scr.p) cudaFree(scr.p);
     scr.p = nullptr;
@@ -737,10 +746,6 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   int *d_err = reinterpret_cast<int *>(base + codes_bytes + std::max(pa.bytes, pb.bytes));
 
   const size_t rsmem = (size_t)SQ_WARPS * sq_region(K) * sizeof(HeapNode);
-  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_prefix, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
-  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_tail, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)rsmem));
-  FKNN_CUDA(cudaFuncSetAttribute(k_sq8_screen, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sizeof(SqScreenSmem)));
   FKNN_CUDA(cudaMemsetAsync(d_err, 0, sizeof(int), st));
   // |c|^2 of every code (the replay kernels use it too) and the tiles
   k_sq8_tiles<<<nct_all, 256, 0, st>>>(d_codes, npoints, 0, 0, ctiles, cncc);
