@@ -162,8 +162,9 @@ int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, u
  * all counters it reads).  Calls that overlap on the GPU (other streams,
  * other host threads, same device) race on that array: serialise them.  The
  * first call on a device looks up the array's device address (set-up once
- * per device), so make that first call before any stream capture begins.
- * The call waits for its stream before returning (the count is read back). */
+ * per device).  Every call waits for its stream before returning (the count
+ * is read back into host memory), so it cannot be issued on a stream that is
+ * being captured into a CUDA graph. */
 int fknn_filter_rows_noalloc(const float *labels, const float *ts, uint64_t n, const float *meta4,
                              uint32_t *out_ids, uint64_t *count, void *stream);
 
@@ -184,9 +185,15 @@ int fknn_sq8_sym_encode(const float *vecs, uint64_t n, float alpha, int8_t *code
  * row in the reference's heap-array order.  dim and alpha are ignored, as in
  * the reference.  Requires 1 <= k <= 2048 and k <= npoints < 2^31.  Pointers
  * may be host or device memory (device codes and queries 16-byte aligned are
- * read in place, after the work queued on the legacy default stream).  The
- * call is synchronous and reentrant: each calling host thread has its own
- * device scratch and stream, kept between calls. */
+ * read in place, after the work queued on the legacy default stream; work
+ * that produced them on a non-blocking stream or a per-thread default stream
+ * must be synchronised by the caller first).  The call is synchronous and
+ * reentrant: each calling host thread has its own device scratch and stream,
+ * kept between calls and only grown.  That scratch holds about
+ * npoints x 132 bytes (plus npoints x 112 when the codes are host memory)
+ * and npoints x k / 512 bytes per query of a pass (up to 8,192 queries), so
+ * it scales with the number of calling threads; release it with
+ * fknn_sq8_release_thread_scratch. */
 int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoints, const char *codes_in,
                         float alpha, size_t nqueries, const int8_t *queries_in);
 
@@ -194,6 +201,11 @@ int fknn_sq8_bruteforce(size_t dim, size_t k, int *closest_points, size_t npoint
  * distances[k] = heap distance * alpha * alpha. */
 int fknn_sq8_bruteforce_subgraph(size_t dim, size_t k, int *closest_points, float *distances, size_t npoints,
                                  const char *codes_in, float alpha, size_t nqueries, const int8_t *queries_in);
+
+/* Frees the calling thread's SQ8 brute-force scratch (device memory, stream
+ * and event; no reference counterpart: the reference holds no device
+ * state).  The next call on the thread sets them up again. */
+int fknn_sq8_release_thread_scratch(void);
 
 /* FP32 re-rank of candidate lists (hybrid_graph.cpp:216-228, 284-296,
  * 481-492: approximate candidates re-scored in FP32, the k best kept).

@@ -126,6 +126,38 @@ def count_matches(labels, ts, metas) -> np.ndarray:
     return out
 
 
+def _sortable(f: np.ndarray) -> np.ndarray:
+    """Order-preserving uint32 image of float32 (-0 folded onto +0)."""
+    u = (np.asarray(f, dtype=np.float32) + np.float32(0.0)).view(np.uint32).astype(np.uint64)
+    return np.where(u & 0x80000000, (~u) & 0xFFFFFFFF, u | 0x80000000)
+
+
+def count_matches_sorted(labels, ts, metas) -> np.ndarray:
+    """The passing-row count of each predicate (type, v, l, r) of
+    utils.h:98-137 -- type 0 all rows, 1 int32(label) == int32(v),
+    2 l <= ts <= r, 3 both -- from binary searches on sorted columns
+    (the counts equal count_matches'; this form costs O((N + Q) log N),
+    so it serves N = 1e7 with Q = 1e6)."""
+    labels, ts, metas = _c(labels, np.float32), _c(ts, np.float32), _c(metas, np.float32)
+    n = labels.shape[0]
+    lab = labels.astype(np.int32).astype(np.int64)
+    t_sorted = np.sort(ts)
+    key = ((lab + (1 << 31)).astype(np.uint64) << np.uint64(32)) | _sortable(ts)
+    key.sort()
+    typ = metas[:, 0].astype(np.int64)
+    out = np.zeros(metas.shape[0], dtype=np.int64)
+    out[typ == 0] = n
+    m2 = typ == 2
+    out[m2] = np.searchsorted(t_sorted, metas[m2, 3], "right") - np.searchsorted(t_sorted, metas[m2, 2], "left")
+    m13 = (typ == 1) | (typ == 3)
+    v = (metas[m13, 1].astype(np.int32).astype(np.int64) + (1 << 31)).astype(np.uint64) << np.uint64(32)
+    t1 = typ[m13] == 1
+    lo = np.where(t1, v, v | _sortable(metas[m13, 2]))
+    hi = np.where(t1, v | np.uint64(0xFFFFFFFF), v | _sortable(metas[m13, 3]))
+    out[m13] = np.searchsorted(key, hi, "right") - np.searchsorted(key, lo, "left")
+    return np.maximum(out, 0).astype(np.uint32)
+
+
 def sq8_sym_train(vecs):
     vecs = _c(vecs, np.float32)
     a = lib().oracle_sq8_sym_alpha(vecs.ctypes.data, vecs.size)

@@ -1299,13 +1299,17 @@ static int noalloc_scratch(uint32_t **out) {
   return FKNN_OK;
 }
 
-static bool on_device(const void *p) {
+// True for device memory of device `dev` and for managed memory; false for
+// host memory and for another GPU's memory (its kernels would read a peer's
+// memory, which faults without peer access).
+static bool on_device(const void *p, int dev) {
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return true;
+  return a.type == cudaMemoryTypeDevice && a.device == dev;
 }
 
 }  // namespace fknn
@@ -1334,7 +1338,9 @@ extern "C" int fknn_filter_rows_noalloc(const float *labels, const float *ts, ui
   }
   *count = 0;
   if (n == 0) return FKNN_OK;
-  if (!on_device(labels) || !on_device(ts) || !on_device(out_ids)) {
+  int cur = 0;
+  FKNN_CUDA(cudaGetDevice(&cur));
+  if (!on_device(labels, cur) || !on_device(ts, cur) || !on_device(out_ids, cur)) {
     set_error("fknn_filter_rows_noalloc: labels, ts and out_ids must be device memory of the current device");
     return FKNN_EINVAL;
   }

@@ -844,4 +844,10 @@ int fknn_sq8_bruteforce_subgraph(size_t dim, size_t k, int *closest_points, floa
   return sq8_bf_impl(k, closest_points, distances, npoints, codes_in, alpha, nqueries, queries_in);
 }
 
+int fknn_sq8_release_thread_scratch(void) {
+  // the thread's stream has no work left: every SQ8 call waits for it
+  sq8_scratch().release();
+  return FKNN_OK;
+}
+
 }  // extern "C"

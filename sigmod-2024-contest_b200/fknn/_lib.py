@@ -139,6 +139,7 @@ SIGNATURES = {
     "fknn_sq8_bruteforce": (c_int, [c_size_t, c_size_t, c_void_p, c_size_t, c_void_p, c_float, c_size_t, c_void_p]),
     "fknn_sq8_bruteforce_subgraph": (c_int, [c_size_t, c_size_t, c_void_p, c_void_p, c_size_t, c_void_p, c_float,
                                              c_size_t, c_void_p]),
+    "fknn_sq8_release_thread_scratch": (c_int, []),
     "fknn_rerank": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_uint32, c_uint32, c_void_p, c_void_p,
                             c_void_p]),
     "fknn_graph_create": (c_int, [c_void_p, c_size_t, c_void_p, c_int, POINTER(c_void_p)]),

@@ -13,7 +13,8 @@ import pytest
 import oracle
 from fknn import datagen
 
-REF_ROOT = "/root/reference"
+# where the reference sources lie (only the recipes that compile or read them use this)
+REF_ROOT = os.environ.get("REF_ROOT", "/root/reference")
 
 
 def _digest(*arrays):
@@ -34,6 +35,18 @@ def test_exact_matches_reference_fixture(golden_dir, name):
     ids, dists = oracle.exact_knn(vecs, labels, ts, q[sel], metas[sel])
     np.testing.assert_array_equal(ids, f["gt"])
     assert np.all(np.diff(dists, axis=1) >= 0)
+
+
+@pytest.mark.parametrize("cfg", [1, 3, 4])
+def test_count_matches_sorted_equals_scan(cfg):
+    """The sorted-column count (used at N = 1e7) equals the row scan,
+    including windows whose bounds fall exactly on row timestamps."""
+    vecs, labels, ts, q, metas = datagen.make_workload(cfg, n=40_000, nq=4_000)
+    hit = np.nonzero(metas[:, 0] >= 2)[0][:100]
+    metas[hit, 2] = ts[hit]
+    metas[hit[::2], 3] = ts[hit[::2]]
+    np.testing.assert_array_equal(oracle.count_matches_sorted(labels, ts, metas),
+                                  oracle.count_matches(labels, ts, metas))
 
 
 def test_exact_ties_match_reference_fixture(golden_dir):

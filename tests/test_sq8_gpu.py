@@ -151,3 +151,26 @@ def test_bruteforce_rejects_bad_k():
     out = np.empty(11, np.int32)
     with pytest.raises(fknn.FknnError):
         fknn.bruteforce(100, 11, out, 10, codes, 1.0, 1, np.zeros(112, np.int8))
+
+
+def test_release_thread_scratch_then_call_again():
+    """fknn_sq8_release_thread_scratch frees the calling thread's scratch;
+    the next call sets it up again and returns the same heap arrays."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(21)
+    vecs = rng.standard_normal((40000, 100), dtype=np.float32)
+    alpha, codes = oracle.sq8_sym_train(vecs)
+    qv = oracle.sq8_sym_encode(rng.standard_normal((3, 100), dtype=np.float32), alpha)
+    k = 140
+    a = np.empty((3, k), dtype=np.int32)
+    b = np.empty((3, k), dtype=np.int32)
+    fknn.bruteforce(100, k, a, codes.shape[0], codes, alpha, 3, qv)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    assert fknn.load().fknn_sq8_release_thread_scratch() == fknn.FKNN_OK
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 > free0  # the scratch went back to the device
+    fknn.bruteforce(100, k, b, codes.shape[0], codes, alpha, 3, qv)
+    np.testing.assert_array_equal(a, b)
+    assert fknn.load().fknn_sq8_release_thread_scratch() == fknn.FKNN_OK
+    assert fknn.load().fknn_sq8_release_thread_scratch() == fknn.FKNN_OK  # twice is harmless

@@ -55,6 +55,26 @@ def test_noalloc_matches_filter_rows_on_two_calls_in_a_row():
             np.testing.assert_array_equal(got, want)
 
 
+def test_noalloc_calls_allocate_no_device_memory():
+    """After the first call on the device (its one-time address look-up and
+    the kernels' module loading), further calls leave the device's free
+    memory exactly where it was."""
+    torch = pytest.importorskip("torch")
+    vecs, labels, ts, q, metas = datagen.make_workload(1, n=200_003, nq=8)
+    labels_d = torch.from_numpy(labels).cuda()
+    ts_d = torch.from_numpy(ts).cuda()
+    out_d = torch.empty(labels.shape[0], dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream().cuda_stream
+    call_noalloc(labels_d, ts_d, labels.shape[0], metas[0], out_d, stream)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    for i in range(6):
+        call_noalloc(labels_d, ts_d, labels.shape[0], metas[i % 8], out_d, stream)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0, f"free device memory moved by {free0 - free1} bytes"
+
+
 def test_noalloc_rejects_sizes_beyond_its_limit_and_host_pointers():
     torch = pytest.importorskip("torch")
     lib = fknn.load()
