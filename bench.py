@@ -499,45 +499,55 @@ def run_graph(args):
     idx.close()
 
 
-def filter_measure(idx, metas, n: int, warmup: int, reps: int) -> dict:
-    """fknn_filter_rows (predicate + compaction) over the resident columns
-    for each predicate in metas: CUDA events around each call on its stream;
-    algorithmic bytes 8 B per row (int32 label + float32 timestamp) plus 4 B
-    per passing row written."""
-    import ctypes
-
+def filter_measure(idx, metas, labels, ts, warmup: int, reps: int, batches=(1, 8)) -> dict:
+    """fknn_filter_rows_batch (predicate + compaction, device-side counts)
+    over the resident columns, the workload's predicates taken P at a time
+    for each P in batches.  Every timed call is preceded by a 256 MB write
+    that flushes L2 (the columns, 8 B per row, fit in it at N = 1e7) and is
+    timed alone by CUDA events on its stream.  Algorithmic bytes per call:
+    8 B per row (int32 label + float32 timestamp, read once for the P
+    predicates) plus 4 B per passing row written.  The counts are checked
+    against the oracle's sorted-column count."""
     import torch
 
-    from fknn import _lib
-    lib = _lib.load()
-    out = torch.empty(n, dtype=torch.int32, device="cuda")
+    import oracle
+    n = int(labels.shape[0])
     stream = torch.cuda.current_stream()
-    cnt = ctypes.c_uint64()
-    rows = []
-    for i in range(metas.shape[0]):
-        m4 = np.ascontiguousarray(metas[i], dtype=np.float32)
-        for rep in range(warmup + reps):
-            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            e0.record(stream)
-            _lib.check(lib.fknn_filter_rows(idx._h, m4.ctypes.data, out.data_ptr(), ctypes.byref(cnt),
-                                            stream.cuda_stream))
-            e1.record(stream)
-            e1.synchronize()
-            if rep >= warmup:
-                rows.append((int(m4[0]), int(cnt.value), e0.elapsed_time(e1)))
-    del out
-    ms = np.array([r[2] for r in rows])
-    byts = np.array([8.0 * n + 4.0 * r[1] for r in rows])
-    gbs = byts.sum() / (ms.sum() * 1e-3) / 1e9
+    flush = torch.empty(64 << 20, dtype=torch.int32, device="cuda")
+    want = oracle.count_matches_sorted(labels, ts, metas)
     peaks = measured_peaks()
     pk = peaks.get("hbm_gbs", 6650.0)
-    per_type = {t: float(np.mean([r[2] for r in rows if r[0] == t])) for t in range(4) if any(r[0] == t for r in rows)}
-    return {"value": gbs, "unit": "GB/s", "peak": pk, "frac": gbs / pk, "kernel": "fknn_filter_rows",
-            "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" [fallback]" if peaks.get("fallback") else ""),
-            "predicates": int(metas.shape[0]), "calls": len(rows), "ms_per_call_mean": float(ms.mean()),
-            "ms_per_call_by_type": per_type,
-            "algorithmic": "8 B per row (label + timestamp) + 4 B per passing row",
-            "passing_rows_mean": float(np.mean([r[1] for r in rows]))}
+    res = {"kernels": ["k_filter_mark", "k_filter_emit"], "unit": "GB/s", "peak": pk,
+           "peak_source": "MEASURED_PEAKS.json hbm_gbs" + (" [fallback]" if peaks.get("fallback") else ""),
+           "algorithmic": "8 B per row (label + timestamp, once per call) + 4 B per passing row",
+           "l2": "flushed (256 MB write) before every timed call", "counts_equal_oracle": True}
+    for P in batches:
+        out = torch.empty((P, n), dtype=torch.int32, device="cuda")
+        counts = torch.empty(P, dtype=torch.int64, device="cuda")
+        ms, byts = [], []
+        for g0 in range(0, metas.shape[0] - P + 1, P):
+            g = np.ascontiguousarray(metas[g0:g0 + P])
+            for rep in range(warmup + reps):
+                flush.zero_()
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(stream)
+                idx.filter_rows_batch(g, out, counts, stream.cuda_stream)
+                e1.record(stream)
+                e1.synchronize()
+                c = counts.cpu().numpy()
+                if not np.array_equal(c, want[g0:g0 + P].astype(np.int64)):
+                    res["counts_equal_oracle"] = False
+                if rep >= warmup:
+                    ms.append(e0.elapsed_time(e1))
+                    byts.append(8.0 * n + 4.0 * float(c.sum()))
+        gbs = float(np.sum(byts) / (np.sum(ms) * 1e-3) / 1e9)
+        res[f"p{P}"] = {"value": gbs, "frac": gbs / pk, "calls": len(ms), "ms_per_call_mean": float(np.mean(ms)),
+                        "passing_rows_mean_per_predicate": float(np.mean(byts) - 8.0 * n) / 4.0 / P}
+        del out, counts
+    res["value"] = res["p1"]["value"]
+    res["frac"] = res["p1"]["frac"]
+    del flush
+    return res
 
 
 def run_filter(args):
@@ -552,7 +562,7 @@ def run_filter(args):
     n = args.n or w.n
     vecs, labels, ts, q, metas = datagen.make_workload(args.config, n=n, nq=64)
     idx = fknn.Index(vecs, labels, ts)
-    r = filter_measure(idx, metas, n, args.warmup, args.steps)
+    r = filter_measure(idx, metas, labels, ts, args.warmup, args.steps)
     print(json.dumps({"mode": "filter", "metric": "predicate compaction HBM GB/s (algorithmic bytes)",
                       "config": {"workload": w.name, "n": n}, **r}), flush=True)
     idx.close()
@@ -868,7 +878,7 @@ def main():
                           for m, stx in (("exact_fp32", st_exact), ("bf16_rerank", st_bf16))},
             "clocks": clk,
         }
-        line["filter"] = filter_measure(idx, metas[:32], n, 1, 3)
+        line["filter"] = filter_measure(idx, metas[:32], labels, ts, 1, 2)
         if world == 1 and not args.no_cpu_baseline:
             line["cpu_baseline"] = cpu_baseline(vecs, labels, ts, q, metas,
                                                 args.cpu_sample or default_cpu_sample(n))

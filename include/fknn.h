@@ -39,7 +39,9 @@ extern "C" {
 #define FKNN_EINVAL (-1)      /* bad argument: shape, query type, non-finite value, k */
 #define FKNN_ENOMEM (-2)      /* device or host allocation failed, or over the HBM budget */
 #define FKNN_ECUDA (-3)       /* a CUDA runtime call failed */
-#define FKNN_ETIMEOUT (-4)    /* a bounded device wait gave up */
+#define FKNN_ETIMEOUT (-4)    /* a bounded device wait (about a second) gave up; fknn_search and
+                                 fknn_sq8_bruteforce* still return complete results: the queries
+                                 it touched were answered again by the exact row scan */
 #define FKNN_EUNSUPPORTED (-5) /* mode not built into this index */
 #define FKNN_ENODEV (-6)      /* no CUDA device */
 
@@ -130,6 +132,13 @@ int fknn_search(fknn_index *index, const float *qvecs, const float *metas, uint3
 int fknn_index_set_tuning(fknn_index *index, int mode, const fknn_tuning *t);
 int fknn_index_get_tuning(const fknn_index *index, int mode, fknn_tuning *t);
 
+/* Test hook for the failure path (no reference counterpart): the next
+ * BF16 / FP8 search on the index issues no row-block copy for its first
+ * work item, so that item's bounded device waits run out after about a
+ * second; the search returns FKNN_ETIMEOUT with complete results, and the
+ * hook is off again for the search after it. */
+int fknn_index_test_withhold_copy(fknn_index *index);
+
 /* As fknn_search with options and statistics (stats may be NULL). */
 int fknn_search_ex(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k,
                    const fknn_search_opts *opts, uint32_t *ids, float *dists, void *stream,
@@ -143,6 +152,15 @@ int fknn_count_matches(fknn_index *index, const float *metas, uint32_t nq, uint3
  * predicate (type, v, l, r): writes the ids of passing rows in increasing
  * order into out_ids (capacity n) and their number into *count. */
 int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, uint64_t *count, void *stream);
+
+/* As fknn_filter_rows for np predicates at once (metas np x 4 float32, host
+ * memory), asynchronous: the columns are read once for up to 16 predicates
+ * per pass, row p of out_ids (DEVICE memory, np x n uint32, row stride n)
+ * receives predicate p's passing ids in increasing order and counts[p]
+ * (DEVICE memory, np uint64) their number.  Nothing is read back; results
+ * are complete when `stream` reaches the point of the call. */
+int fknn_filter_rows_batch(fknn_index *index, const float *metas, uint32_t np, uint32_t *out_ids,
+                           uint64_t *counts, void *stream);
 
 /* No counterpart in the reference: the predicate evaluation + row compaction
  * of fknn_filter_rows for callers that cannot allocate device memory -- code

@@ -132,6 +132,21 @@ def _sortable(f: np.ndarray) -> np.ndarray:
     return np.where(u & 0x80000000, (~u) & 0xFFFFFFFF, u | 0x80000000)
 
 
+def filter_rows(labels, ts, meta4) -> np.ndarray:
+    """Ids (increasing, uint32) of the rows passing one predicate (type, v,
+    l, r) of utils.h:110-137: type 0 every row, 1 int32(label) == int32(v),
+    2 l <= ts <= r, 3 both."""
+    labels, ts = _c(labels, np.float32), _c(ts, np.float32)
+    m = np.asarray(meta4, dtype=np.float32).reshape(4)
+    t = int(np.uint32(m[0]))
+    keep = np.ones(labels.shape[0], dtype=bool)
+    if t in (1, 3):
+        keep &= labels.astype(np.int32) == np.int32(m[1])
+    if t in (2, 3):
+        keep &= (ts >= m[2]) & (ts <= m[3])
+    return np.nonzero(keep)[0].astype(np.uint32)
+
+
 def count_matches_sorted(labels, ts, metas) -> np.ndarray:
     """The passing-row count of each predicate (type, v, l, r) of
     utils.h:98-137 -- type 0 all rows, 1 int32(label) == int32(v),

@@ -410,7 +410,8 @@ __global__ void __launch_bounds__(B_THREADS, 2)
                   const float2 *__restrict__ lane_qs, const unsigned char *__restrict__ blocks_t,
                   const unsigned char *__restrict__ blocks_c, uint32_t *__restrict__ T_global,
                   uint32_t *__restrict__ ovf, Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt,
-                  uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride, int *err) {
+                  uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride, uint32_t withhold,
+                  int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   BScreenSmem<F> &sm = *reinterpret_cast<BScreenSmem<F> *>(smem_raw);
   constexpr uint32_t TB = Tiles<F>::BYTES;
@@ -450,7 +451,10 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       mbar_arrive_expect_tx(&sm.abar, TB);
       bulk_g2s(sm.a, atiles + (uint64_t)it.tile * TB, TB, &sm.abar);
       uint32_t issued = 0;
-      for (uint32_t sub = 0; sub < nsub; ++sub) {
+      // test hook (fknn_index_test_withhold_copy): the first work item issues
+      // no row-block copy, so its MMA issuer's and epilogue's waits run out
+      const uint32_t nsub_issue = (withhold && item_id == 0) ? 0u : nsub;
+      for (uint32_t sub = 0; sub < nsub_issue; ++sub) {
         const int st = sub % BS;
         if (sub >= BS && !mbar_wait_bounded(&sm.empty[st], ((sub / BS) - 1) & 1, err)) break;
         mbar_arrive_expect_tx(&sm.full[st], TB);
@@ -963,7 +967,7 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
           (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at,
           (const int32_t *)(d_blob + o_lq), (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le),
           d_lqs, (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A,
-          d_out, d_ocnt, r, capb, 0, stride, idx->d_flag);
+          d_out, d_ocnt, r, capb, 0, stride, 0u, idx->d_flag);
       k_seed_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>((nbig + 255) / 256, 1184)), 256, 0, st>>>(
           (const uint32_t *)(d_blob + o_big), nbig, d_desc, T_A, ovf_A, 16 * stride * BR, T_global, seeded);
       g_launches += 3;
@@ -972,7 +976,8 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
         (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_lqs,
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
-        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->d_flag);
+        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->test_withhold ? 1u : 0u, idx->d_flag);
+    idx->test_withhold = false;
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     MergeArgs A;
     A.big_q = (const uint32_t *)(d_blob + o_big);

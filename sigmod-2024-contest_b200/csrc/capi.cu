@@ -345,10 +345,20 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
   int flag = 0;
   FKNN_CUDA(cudaMemcpyAsync(&flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
-  if (flag & (1 << 8)) {
-    set_error("fknn_search: a bounded device wait gave up; affected queries were answered by the exact scan");
-  }
   if (stats) stats->kernel_launches = g_launches;
+  if (flag & (1 << 8)) {
+    // the outputs are complete: the affected queries were re-answered by the
+    // exact scan; the status tells the caller that a device wait gave up
+    set_error("fknn_search: a bounded device wait gave up; affected queries were answered by the exact scan");
+    return FKNN_ETIMEOUT;
+  }
+  return FKNN_OK;
+}
+
+int fknn_index_test_withhold_copy(fknn_index *index) {
+  if (!index) return FKNN_EINVAL;
+  std::lock_guard<std::mutex> lock(index->mu);
+  index->test_withhold = true;
   return FKNN_OK;
 }
 
@@ -419,15 +429,11 @@ int fknn_filter_rows(fknn_index *idx, const float *meta4, uint32_t *out_ids, uin
   g_err.clear();
   g_launches = 0;
   if (!idx || !meta4 || !out_ids || !count) return FKNN_EINVAL;
-  const float t = meta4[0];
-  if (!(t == 0.f || t == 1.f || t == 2.f || t == 3.f)) {
-    set_error("fknn_filter_rows: query type not in {0,1,2,3}");
-    return FKNN_EINVAL;
-  }
+  int rc;
+  if ((rc = filter_check_preds(meta4, 1, "fknn_filter_rows"))) return rc;
   std::lock_guard<std::mutex> lock(idx->mu);
   FKNN_CUDA(cudaSetDevice(idx->device));
   cudaStream_t st = (cudaStream_t)stream;
-  int rc;
   uint32_t *d_out = out_ids;
   const bool o_dev = is_device_ptr(out_ids);
   if (!o_dev)
@@ -436,6 +442,26 @@ int fknn_filter_rows(fknn_index *idx, const float *meta4, uint32_t *out_ids, uin
   if (!o_dev && *count) FKNN_CUDA(cudaMemcpyAsync(out_ids, d_out, *count * 4, cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
   return FKNN_OK;
+}
+
+int fknn_filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t *out_ids, uint64_t *counts,
+                           void *stream) {
+  g_err.clear();
+  g_launches = 0;
+  if (!idx || !metas || !out_ids || !counts) {
+    set_error("fknn_filter_rows_batch: NULL argument");
+    return FKNN_EINVAL;
+  }
+  int rc;
+  if ((rc = filter_check_preds(metas, np, "fknn_filter_rows_batch"))) return rc;
+  if (np == 0) return FKNN_OK;
+  std::lock_guard<std::mutex> lock(idx->mu);
+  FKNN_CUDA(cudaSetDevice(idx->device));
+  if (!is_device_ptr(out_ids) || !is_device_ptr(counts)) {
+    set_error("fknn_filter_rows_batch: out_ids and counts must be device memory");
+    return FKNN_EINVAL;
+  }
+  return filter_rows_batch(idx, metas, np, out_ids, counts, (cudaStream_t)stream);
 }
 
 int fknn_bruteforce_rows(const float *nodes, uint32_t n, const float *queries, uint32_t nq, uint32_t *gt) {

@@ -6,8 +6,11 @@
 
 namespace fknn {
 
-// Iteration cap for every spin-wait (~ a second or two at B200 clocks).
-constexpr uint32_t WAIT_LIMIT = 1u << 26;
+// Every spin-wait gives up after WAIT_NS nanoseconds of the global timer
+// (checked every 64 polls), with an iteration cap behind it in case the
+// timer does not advance.
+constexpr uint64_t WAIT_NS = 1000000000ull;
+constexpr uint32_t WAIT_LIMIT = 1u << 28;
 
 // Error bits written to the per-call device flag.
 constexpr int ERR_WAIT_TIMEOUT = 1 << 8;
@@ -56,11 +59,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity) {
   return ok != 0;
 }
 
+__device__ __forceinline__ uint64_t global_ns() {
+  uint64_t t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+
 // Bounded wait: returns false (and raises ERR_WAIT_TIMEOUT) if the phase
-// never completes.
+// has not completed within WAIT_NS.
 __device__ __forceinline__ bool mbar_wait_bounded(uint64_t *bar, uint32_t parity, int *err) {
-  for (uint32_t it = 0; it < WAIT_LIMIT; ++it)
+  if (mbar_try_wait(bar, parity)) return true;
+  const uint64_t t0 = global_ns();
+  for (uint32_t it = 0; it < WAIT_LIMIT; ++it) {
     if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 63u) == 63u && global_ns() - t0 > WAIT_NS) break;
+  }
   atomicOr(err, ERR_WAIT_TIMEOUT);
   return false;
 }

@@ -612,7 +612,11 @@ __global__ void __launch_bounds__(ES_THREADS)
   }
 }
 
-// ------------------------------------------------- predicate compaction --
+// ------------------------------------ predicate compaction (no-alloc form) --
+//
+// Count -> scan -> write over 4,096-row tiles: its only scratch is one
+// counter per tile, which fits the fixed array of fknn_filter_rows_noalloc.
+// The index's fknn_filter_rows / fknn_filter_rows_batch use filter.cu.
 
 constexpr int FC_THREADS = 256;
 constexpr int FC_ITEMS = 16;
@@ -781,24 +785,6 @@ int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d
                                            idx->ord[ORDER_CAT].label, idx->ord[ORDER_CAT].ts, d_counts);
   g_launches += 1;
   FKNN_CUDA(cudaGetLastError());
-  return FKNN_OK;
-}
-
-int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *count, cudaStream_t st) {
-  const uint64_t n = idx->n;
-  const uint32_t ntiles = (uint32_t)((n + FC_TILE - 1) / FC_TILE);
-  uint32_t *tc;
-  int rc = ws_get(idx, 10, (size_t)(ntiles + 1) * 4, (void **)&tc);
-  if (rc) return rc;
-  const float4 m = make_float4(m4[0], m4[1], m4[2], m4[3]);
-  k_filter_count<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc);
-  k_exclusive_scan_small<<<1, 1024, 0, st>>>(tc, ntiles, tc + ntiles);
-  k_filter_write<<<ntiles, FC_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, m, tc, d_out);
-  g_launches += 3;
-  uint32_t tot = 0;
-  FKNN_CUDA(cudaMemcpyAsync(&tot, tc + ntiles, 4, cudaMemcpyDeviceToHost, st));
-  FKNN_CUDA(cudaStreamSynchronize(st));
-  *count = tot;
   return FKNN_OK;
 }
 

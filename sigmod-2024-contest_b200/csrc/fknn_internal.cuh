@@ -205,7 +205,7 @@ struct fknn_index {
   float *fp8_scale = nullptr;
   // per-call scratch
   std::mutex mu;
-  fknn::DevBuf ws[16];
+  fknn::DevBuf ws[19];
   fknn::HostBuf hs[8];
   int *d_flag = nullptr;
   cudaStream_t own_stream = nullptr;
@@ -219,6 +219,8 @@ struct fknn_index {
   // a view shares the device data of another index and owns only its
   // per-call scratch (ws, hs, d_flag), so views search concurrently
   bool is_view = false;
+  // test hook: the next reduced-precision search withholds one row-block copy
+  bool test_withhold = false;
 };
 
 namespace fknn {
@@ -250,6 +252,10 @@ int radix_sort_pairs(fknn_index *idx, uint32_t *keys, uint32_t *vals, uint32_t *
 int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
                  float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d_counts, cudaStream_t st);
+// predicate compaction (filter.cu): host predicates, device outputs
+int filter_check_preds(const float *metas_host, uint32_t np, const char *who);
+int filter_rows_batch(fknn_index *idx, const float *metas_host, uint32_t np, uint32_t *d_out, uint64_t *d_counts,
+                      cudaStream_t st);
 int filter_rows(fknn_index *idx, const float *meta4_host, uint32_t *d_out, uint64_t *count, cudaStream_t st);
 int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st);
 int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,

@@ -794,8 +794,11 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   int err = 0;
   FKNN_CUDA(cudaMemcpyAsync(&err, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
-  if (err & ERR_WAIT_TIMEOUT)
+  if (err & ERR_WAIT_TIMEOUT) {
+    // outputs are complete (the affected queries took the exact scan)
     set_error("fknn_sq8_bruteforce: a bounded device wait gave up; affected queries were answered by the exact scan");
+    return FKNN_ETIMEOUT;
+  }
   return FKNN_OK;
 }
 

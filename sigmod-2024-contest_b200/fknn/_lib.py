@@ -126,11 +126,13 @@ SIGNATURES = {
     "fknn_index_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
     "fknn_index_set_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),
     "fknn_index_get_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),
+    "fknn_index_test_withhold_copy": (c_int, [c_void_p]),
     "fknn_search": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_int, c_void_p, c_void_p, c_void_p]),
     "fknn_search_ex": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, POINTER(SearchOpts), c_void_p,
                                c_void_p, c_void_p, POINTER(SearchStats)]),
     "fknn_count_matches": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p]),
     "fknn_filter_rows": (c_int, [c_void_p, c_void_p, c_void_p, POINTER(c_uint64), c_void_p]),
+    "fknn_filter_rows_batch": (c_int, [c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),
     "fknn_filter_rows_noalloc": (c_int, [c_void_p, c_void_p, c_uint64, c_void_p, c_void_p, POINTER(c_uint64),
                                          c_void_p]),
     "fknn_bruteforce_rows": (c_int, [c_void_p, c_uint32, c_void_p, c_uint32, c_void_p]),

@@ -195,6 +195,25 @@ class Index:
         check(load().fknn_count_matches(self._h, metas.ctypes.data, metas.shape[0], out.ctypes.data, None))
         return out
 
+    def filter_rows_batch(self, metas, out=None, counts=None, stream: Optional[int] = None):
+        """fknn_filter_rows_batch: the passing ids of each predicate row of
+        metas ((np, 4) host floats), one pass over the columns per 16
+        predicates.  out ((np, n) int32) and counts ((np,) int64) are torch
+        CUDA tensors (allocated when None); returns them, asynchronously
+        written on `stream` (default: torch's current stream)."""
+        import torch
+        m = np.ascontiguousarray(metas, dtype=np.float32).reshape(-1, 4)
+        npred = m.shape[0]
+        if out is None:
+            out = torch.empty((npred, self.n), dtype=torch.int32, device=f"cuda:{self.device}")
+        if counts is None:
+            counts = torch.empty(npred, dtype=torch.int64, device=f"cuda:{self.device}")
+        if stream is None:
+            stream = torch.cuda.current_stream(self.device).cuda_stream
+        check(load().fknn_filter_rows_batch(self._h, m.ctypes.data, npred, out.data_ptr(), counts.data_ptr(),
+                                            stream))
+        return out, counts
+
     def filter_rows(self, meta4) -> np.ndarray:
         """Ids of the rows passing one predicate (type, v, l, r), increasing."""
         m = np.ascontiguousarray(meta4, dtype=np.float32).reshape(4)

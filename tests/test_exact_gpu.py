@@ -162,6 +162,32 @@ def test_filter_rows_many_tiles():
             np.testing.assert_array_equal(got, np.nonzero(keep)[0].astype(np.uint32))
 
 
+@pytest.mark.parametrize("n", [100, 4096, 1_000_003])
+def test_filter_rows_batch_matches_oracle(n):
+    """fknn_filter_rows_batch: 21 predicates in one call (two passes of at
+    most 16), every query type, an empty result, exact-boundary windows and
+    a row count that is not a multiple of the chunk; ids and device counts
+    equal the oracle's, and the single-predicate call agrees."""
+    torch = pytest.importorskip("torch")
+    vecs, labels, ts, q, metas = datagen.make_workload(4, n=n, nq=17)
+    extra = np.array([[1, 99_999, -1, -1],          # category that no row has
+                      [2, ts[n // 2], ts[n // 2], 0],  # a window of one timestamp
+                      [3, labels[0], 0.0, 1.0],
+                      [0, -1, -1, -1]], np.float32)
+    extra[1, 3] = extra[1, 2]
+    preds = np.concatenate([metas, extra])
+    with fknn.Index(vecs, labels, ts) as idx:
+        out, counts = idx.filter_rows_batch(preds)
+        torch.cuda.synchronize()
+        out_h, counts_h = out.cpu().numpy().view(np.uint32), counts.cpu().numpy()
+        for p in range(preds.shape[0]):
+            want = oracle.filter_rows(labels, ts, preds[p])
+            assert counts_h[p] == len(want), p
+            np.testing.assert_array_equal(out_h[p, :len(want)], want)
+        np.testing.assert_array_equal(idx.filter_rows(preds[2]), oracle.filter_rows(labels, ts, preds[2]))
+    assert counts_h[17] == 0 and counts_h[20] == n and counts_h[18] >= 1
+
+
 def test_invalid_queries_rejected():
     vecs, labels, ts, q, metas = datagen.make_workload(1, n=5000, nq=4)
     with fknn.Index(vecs, labels, ts) as idx:

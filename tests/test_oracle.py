@@ -49,6 +49,17 @@ def test_count_matches_sorted_equals_scan(cfg):
                                   oracle.count_matches(labels, ts, metas))
 
 
+def test_filter_rows_counts_equal_the_c_restatement():
+    """oracle.filter_rows (the predicate as a column mask) passes exactly
+    the rows oracle_count_matches counts, on every query type."""
+    vecs, labels, ts, q, metas = datagen.make_workload(4, n=30_000, nq=400)
+    counts = oracle.count_matches(labels, ts, metas)
+    for i in range(metas.shape[0]):
+        ids = oracle.filter_rows(labels, ts, metas[i])
+        assert len(ids) == counts[i]
+        assert np.all(np.diff(ids.astype(np.int64)) > 0)
+
+
 def test_exact_ties_match_reference_fixture(golden_dir):
     f = np.load(os.path.join(golden_dir, "exact_ties.npz"))
     vecs, labels, ts, q, metas = datagen.make_workload(1, n=400, nq=30)
