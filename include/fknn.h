@@ -107,7 +107,32 @@ const char *fknn_last_error(void);
 int fknn_index_create(const float *vecs, const float *labels, const float *ts, uint64_t n,
                       uint32_t dim, const fknn_index_opts *opts, fknn_index **out);
 
+/* Builds a resident index straight from a contest base file (u32 N, then N
+ * rows [label, ts, 100 floats], as ReadBase reads it, utils.h:257-276):
+ * the rows stream through pinned buffers to the device, a kernel splits
+ * them into the columns, and the row orders that ReadSortedBaseTimestamp
+ * builds with host sorts (utils.h:352-479) are radix-sorted on the GPU.
+ * Row position in the file is the id. */
+int fknn_index_create_from_file(const char *path, const fknn_index_opts *opts, fknn_index **out);
+
 int fknn_index_destroy(fknn_index *index);
+
+/* ---- Contest file formats ----
+ * fknn_read_base_file   <- ReadBase          utils.h:257-276: *n rows; vecs n x 100, labels n, ts n
+ *                          (all three NULL: only *n is set)
+ * fknn_read_query_file  <- ReadQuery         utils.h:550-566: *nq rows; qvecs nq x 100, metas nq x 4
+ *                          (both NULL: only *nq is set)
+ * fknn_sorted_query_order <- the order ReadSortedQuery sorts queries into, utils.h:513-533:
+ *                          ascending (uint32 type, int32 v, l, r); equal keys keep their order
+ * fknn_save_knn         <- SaveKNN           io.h:22-33: nq x k uint32, no header
+ * fknn_read_groundtruth <- ReadGroundTruth   utils.h:194-221: u32 nq header, then nq x k uint32
+ *                          (ids NULL: only *nq is set)
+ * A file shorter than its header says is rejected with FKNN_EINVAL. */
+int fknn_read_base_file(const char *path, uint64_t *n, float *vecs, float *labels, float *ts);
+int fknn_read_query_file(const char *path, uint32_t *nq, float *qvecs, float *metas);
+int fknn_sorted_query_order(const float *metas, uint32_t nq, uint32_t *sorted_ids);
+int fknn_save_knn(const char *path, const uint32_t *ids, uint32_t nq, uint32_t k);
+int fknn_read_groundtruth(const char *path, uint32_t k, uint32_t *nq, uint32_t *ids);
 
 /* Device bytes held by the index. */
 int fknn_index_bytes(const fknn_index *index, uint64_t *bytes);

@@ -15,6 +15,7 @@
 // per-row term left for the epilogue: a row is a candidate for query q iff
 // acc >= (|q|^2 - T_q)/2, one compare per TMEM value.
 #include <algorithm>
+#include <cfloat>
 #include <chrono>
 #include <cstring>
 
@@ -79,15 +80,17 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, 
   }
 }
 
-// max of 32 values as a tree (NaN entries ignored)
+// max of 32 values as a tree of three-input maxima (16 instructions)
 __device__ __forceinline__ float max32(const float *v) {
-  float a[8];
+  float a[10];
 #pragma unroll
-  for (int k = 0; k < 8; ++k) a[k] = fmaxf(fmaxf(v[4 * k], v[4 * k + 1]), fmaxf(v[4 * k + 2], v[4 * k + 3]));
-  return fmaxf(fmaxf(fmaxf(a[0], a[1]), fmaxf(a[2], a[3])), fmaxf(fmaxf(a[4], a[5]), fmaxf(a[6], a[7])));
+  for (int k = 0; k < 10; ++k) a[k] = fmax3(v[3 * k], v[3 * k + 1], v[3 * k + 2]);
+  const float b0 = fmax3(a[0], a[1], a[2]), b1 = fmax3(a[3], a[4], a[5]), b2 = fmax3(a[6], a[7], a[8]);
+  const float b3 = fmax3(a[9], v[30], v[31]);
+  return fmax3(b0, b1, fmaxf(b2, b3));
 }
 
-// bit j set iff v[j] >= t (false for NaN), built as four independent chains
+// bit j set iff v[j] >= t, built as four independent chains
 __device__ __forceinline__ uint32_t ge_mask32(const float *v, float t) {
   uint32_t p[4] = {0u, 0u, 0u, 0u};
 #pragma unroll
@@ -281,6 +284,39 @@ struct BScreenSmem {
 // two screening CTAs share an SM (228 KB of shared memory, 1 KB reserved per CTA)
 static_assert(sizeof(BScreenSmem<FmtBF16>) <= 113 * 1024 && sizeof(BScreenSmem<FmtFP8>) <= 113 * 1024,
               "screen shared memory must leave room for two CTAs per SM");
+
+// Screens 32 accumulator columns c .. c+31 of one query (this lane): every
+// column j inside the slab [r0, r1) with acc >= cq is appended to the
+// query's list with its screening distance qn - 2 sc acc.  The lane's
+// candidates form a bit mask; their values are read back from the lane's
+// shared-memory staging row, so the push loop runs once per candidate.
+__device__ __forceinline__ int screen_chunk(const uint32_t (&r)[32], int c, int r0, int r1, float cq, float qn,
+                                            float sc, uint32_t p0, float *row, Candidate *list, int cnt) {
+  if (r0 >= c + 32 || r1 <= c) return cnt;
+  float v[32];
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
+  if (!(r0 <= c && r1 >= c + 32)) {
+#pragma unroll
+    for (int j = 0; j < 32; ++j)
+      if (c + j < r0 || c + j >= r1) v[j] = -INFINITY;
+  }
+  if (max32(v) >= cq) {
+    uint32_t mask = ge_mask32(v, cq);
+#pragma unroll
+    for (int j = 0; j < 32; j += 4)
+      *reinterpret_cast<float4 *>(row + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      Candidate cd;
+      cd.ds = fmaf(-2.f * sc, row[j], qn);
+      cd.pos = p0 + c + j;
+      list[cnt++] = cd;
+    }
+  }
+  return cnt;
+}
 
 // kth smallest (1-based) of the n keys held NPL per lane (element
 // j*32 + lane in key[j]; keys past n ignored): a warp radix select that
@@ -525,41 +561,29 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       const uint32_t p0 = (it.blk0 + sub * stride) * BR;
       const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
       const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
-      // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc)
-      const float cq = (T == INFINITY) ? -INFINITY : 0.5f * (qn - T) / sc;
-#pragma unroll 1
-      for (int c2 = 0; c2 < BR; c2 += 64) {
-        float v[64];
-        tmem_ld64(tmem + ((uint32_t)(wg * 32) << 16) + ab * BR + c2, v);
-        if (r0 >= c2 + 64 || r1 <= c2) continue;
-        if (!(r0 <= c2 && r1 >= c2 + 64)) {
-          // columns outside this query's slab become NaN: ignored by the max, rejected by every compare
-#pragma unroll
-          for (int j = 0; j < 64; ++j)
-            if (c2 + j < r0 || c2 + j >= r1) v[j] = __int_as_float(0x7fc00000);
-        }
-#pragma unroll
-        for (int h = 0; h < 64; h += 32) {
-          if (max32(v + h) >= cq) {
-            // this lane's candidates as a bit mask; their values are read back
-            // from shared memory, so the push loop runs once per candidate of
-            // the lane with the most, not once per column
-            uint32_t mask = ge_mask32(v + h, cq);
-            float *row = &sm.stage[wslot][lane * STAGE_ROW];
-#pragma unroll
-            for (int j = 0; j < 32; j += 4)
-              *reinterpret_cast<float4 *>(row + j) = make_float4(v[h + j], v[h + j + 1], v[h + j + 2], v[h + j + 3]);
-            while (mask) {
-              const int j = __ffs(mask) - 1;
-              mask &= mask - 1;
-              Candidate cd;
-              cd.ds = fmaf(-2.f * sc, row[j], qn);
-              cd.pos = p0 + c2 + h + j;
-              list[cnt++] = cd;
-            }
-          }
-        }
-      }
+      // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc);
+      // with no bound yet every column of the slab is one (cq = -FLT_MAX),
+      // and columns outside the slab are -inf, which no cq admits
+      const float cq = (T == INFINITY) ? -FLT_MAX : 0.5f * (qn - T) / sc;
+      // four 32-column chunks; the TMEM load of the next chunk is in flight
+      // while this one is screened
+      const uint32_t tb = tmem + ((uint32_t)(wg * 32) << 16) + ab * BR;
+      uint32_t ra[32], rb[32];
+      tmem_ld32_issue(tb, ra);
+      tmem_wait_ld(ra);
+      tmem_ld32_issue(tb + 32, rb);
+      cnt = screen_chunk(ra, 0, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+      __syncwarp();
+      tmem_wait_ld(rb);
+      tmem_ld32_issue(tb + 64, ra);
+      cnt = screen_chunk(rb, 32, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+      __syncwarp();
+      tmem_wait_ld(ra);
+      tmem_ld32_issue(tb + 96, rb);
+      cnt = screen_chunk(ra, 64, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+      __syncwarp();
+      tmem_wait_ld(rb);
+      cnt = screen_chunk(rb, 96, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
       tc_fence_before();
       __syncwarp();
       if (lane == 0) mbar_arrive1(&sm.accempty[ab]);

@@ -1,6 +1,7 @@
 // C ABI entry points (include/fknn.h), error plumbing and device memory.
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <new>
 
 #include "fknn_internal.cuh"
@@ -171,35 +172,12 @@ uint64_t scratch_bytes(const fknn_index *idx) {
   return b;
 }
 
-}  // namespace fknn
-
-using namespace fknn;
-
-extern "C" {
-
-int fknn_version(void) { return 100; }
-
-const char *fknn_last_error(void) { return g_err.c_str(); }
-
-int fknn_index_create(const float *vecs, const float *labels, const float *ts, uint64_t n, uint32_t dim,
-                      const fknn_index_opts *opts, fknn_index **out) {
-  g_err.clear();
-  g_launches = 0;
-  if (!out) {
-    set_error("fknn_index_create: out is NULL");
-    return FKNN_EINVAL;
-  }
-  *out = nullptr;
-  if (dim != (uint32_t)DIM) {
-    set_error("fknn_index_create: dim must be 100");
-    return FKNN_EINVAL;
-  }
+// Device set-up, the row columns and orders (build), the reduced-precision
+// copies the options ask for, then the build temporaries are released.
+int create_index(uint64_t n, const fknn_index_opts *opts,
+                 const std::function<int(fknn_index *, cudaStream_t)> &build, fknn_index **out) {
   if (n == 0 || n >= (1ull << 31)) {
     set_error("fknn_index_create: n must be in [1, 2^31)");
-    return FKNN_EINVAL;
-  }
-  if (!vecs || !labels || !ts) {
-    set_error("fknn_index_create: NULL input column");
     return FKNN_EINVAL;
   }
   int ndev = 0;
@@ -233,7 +211,7 @@ int fknn_index_create(const float *vecs, const float *labels, const float *ts, u
     e = cudaMalloc(&idx->d_flag, 64);
     if (e != cudaSuccess) rc = cuda_fail(e, "cudaMalloc");
   }
-  if (!rc) rc = build_index(idx, vecs, labels, ts, idx->own_stream);
+  if (!rc) rc = build(idx, idx->own_stream);
   if (!rc && opts && opts->build_bf16) {
     rc = build_bf16(idx, idx->own_stream);
     if (!rc) {
@@ -263,6 +241,37 @@ int fknn_index_create(const float *vecs, const float *labels, const float *ts, u
   }
   *out = idx;
   return FKNN_OK;
+}
+
+}  // namespace fknn
+
+using namespace fknn;
+
+extern "C" {
+
+int fknn_version(void) { return 100; }
+
+const char *fknn_last_error(void) { return g_err.c_str(); }
+
+int fknn_index_create(const float *vecs, const float *labels, const float *ts, uint64_t n, uint32_t dim,
+                      const fknn_index_opts *opts, fknn_index **out) {
+  g_err.clear();
+  g_launches = 0;
+  if (!out) {
+    set_error("fknn_index_create: out is NULL");
+    return FKNN_EINVAL;
+  }
+  *out = nullptr;
+  if (dim != (uint32_t)DIM) {
+    set_error("fknn_index_create: dim must be 100");
+    return FKNN_EINVAL;
+  }
+  if (!vecs || !labels || !ts) {
+    set_error("fknn_index_create: NULL input column");
+    return FKNN_EINVAL;
+  }
+  return create_index(n, opts, [&](fknn_index *idx, cudaStream_t st) { return build_index(idx, vecs, labels, ts, st); },
+                      out);
 }
 
 int fknn_index_destroy(fknn_index *index) {

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <functional>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -235,6 +236,9 @@ int cuda_fail(cudaError_t e, const char *what);
   } while (0)
 
 int dev_alloc(fknn_index *idx, void **p, size_t bytes);
+// index creation around a column builder (capi.cu)
+int create_index(uint64_t n, const fknn_index_opts *opts,
+                 const std::function<int(fknn_index *, cudaStream_t)> &build, fknn_index **out);
 // search views of one index (capi.cu)
 int make_index_view(fknn_index *base, fknn_index **out);
 void destroy_index(fknn_index *idx);
@@ -245,6 +249,9 @@ int hs_get(fknn_index *idx, int slot, size_t bytes, void **p);
 
 // index build (index_build.cu)
 int build_index(fknn_index *idx, const float *vecs, const float *labels, const float *ts, cudaStream_t st);
+// the same after the columns (vecs, labels_f, ts_f) are on the device
+int alloc_index_columns(fknn_index *idx);
+int build_index_from_columns(fknn_index *idx, cudaStream_t st);
 int radix_sort_pairs(fknn_index *idx, uint32_t *keys, uint32_t *vals, uint32_t *keys_tmp, uint32_t *vals_tmp,
                      uint64_t n, int begin_bit, int end_bit, cudaStream_t st);
 

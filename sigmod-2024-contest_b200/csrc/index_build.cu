@@ -219,21 +219,29 @@ int radix_sort_pairs(fknn_index *idx, uint32_t *keys, uint32_t *vals, uint32_t *
   return FKNN_OK;
 }
 
+int alloc_index_columns(fknn_index *idx) {
+  const uint64_t n = idx->n;
+  int rc;
+  if ((rc = dev_alloc(idx, (void **)&idx->vecs, n * DIM * sizeof(float)))) return rc;
+  if ((rc = dev_alloc(idx, (void **)&idx->norms, n * sizeof(float)))) return rc;
+  if ((rc = dev_alloc(idx, (void **)&idx->labels_f, n * sizeof(float)))) return rc;
+  if ((rc = dev_alloc(idx, (void **)&idx->ts_f, n * sizeof(float)))) return rc;
+  return FKNN_OK;
+}
+
 int build_index(fknn_index *idx, const float *h_vecs, const float *h_labels, const float *h_ts, cudaStream_t st) {
   const uint64_t n = idx->n;
   int rc;
-  rc = dev_alloc(idx, (void **)&idx->vecs, n * DIM * sizeof(float));
-  if (rc) return rc;
-  rc = dev_alloc(idx, (void **)&idx->norms, n * sizeof(float));
-  if (rc) return rc;
-  rc = dev_alloc(idx, (void **)&idx->labels_f, n * sizeof(float));
-  if (rc) return rc;
-  rc = dev_alloc(idx, (void **)&idx->ts_f, n * sizeof(float));
-  if (rc) return rc;
+  if ((rc = alloc_index_columns(idx))) return rc;
   FKNN_CUDA(cudaMemcpyAsync(idx->vecs, h_vecs, n * DIM * sizeof(float), cudaMemcpyDefault, st));
   FKNN_CUDA(cudaMemcpyAsync(idx->labels_f, h_labels, n * sizeof(float), cudaMemcpyDefault, st));
   FKNN_CUDA(cudaMemcpyAsync(idx->ts_f, h_ts, n * sizeof(float), cudaMemcpyDefault, st));
+  return build_index_from_columns(idx, st);
+}
 
+int build_index_from_columns(fknn_index *idx, cudaStream_t st) {
+  const uint64_t n = idx->n;
+  int rc;
   FKNN_CUDA(cudaMemsetAsync(idx->d_flag, 0, sizeof(int), st));
   k_validate_base<<<148 * 8, 256, 0, st>>>(idx->vecs, idx->labels_f, idx->ts_f, n, idx->d_flag);
   int flag = 0;

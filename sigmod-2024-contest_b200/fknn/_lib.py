@@ -122,7 +122,13 @@ SIGNATURES = {
     "fknn_last_error": (c_char_p, []),
     "fknn_index_create": (c_int, [c_void_p, c_void_p, c_void_p, c_uint64, c_uint32, POINTER(IndexOpts),
                                   POINTER(c_void_p)]),
+    "fknn_index_create_from_file": (c_int, [c_char_p, POINTER(IndexOpts), POINTER(c_void_p)]),
     "fknn_index_destroy": (c_int, [c_void_p]),
+    "fknn_read_base_file": (c_int, [c_char_p, POINTER(c_uint64), c_void_p, c_void_p, c_void_p]),
+    "fknn_read_query_file": (c_int, [c_char_p, POINTER(c_uint32), c_void_p, c_void_p]),
+    "fknn_sorted_query_order": (c_int, [c_void_p, c_uint32, c_void_p]),
+    "fknn_save_knn": (c_int, [c_char_p, c_void_p, c_uint32, c_uint32]),
+    "fknn_read_groundtruth": (c_int, [c_char_p, c_uint32, POINTER(c_uint32), c_void_p]),
     "fknn_index_bytes": (c_int, [c_void_p, POINTER(c_uint64)]),
     "fknn_index_set_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),
     "fknn_index_get_tuning": (c_int, [c_void_p, c_int, POINTER(Tuning)]),

@@ -86,6 +86,23 @@ class Index:
         self.n = n
         self.device = device
 
+    @classmethod
+    def from_file(cls, path: str, device: int = 0, build_bf16: bool = False, build_fp8: bool = False,
+                  hbm_budget: int = 0) -> "Index":
+        """fknn_index_create_from_file: a resident index straight from a
+        contest base file (rows streamed to the device and split there)."""
+        lib = load()
+        opts = IndexOpts(device, int(build_bf16), int(build_fp8), hbm_budget)
+        h = c_void_p()
+        check(lib.fknn_index_create_from_file(path.encode(), byref(opts), byref(h)))
+        self = cls.__new__(cls)
+        self._h = h
+        self.device = device
+        nb = c_uint64()
+        check(lib.fknn_read_base_file(path.encode(), byref(nb), None, None, None))
+        self.n = nb.value
+        return self
+
     def close(self) -> None:
         if getattr(self, "_h", None):
             load().fknn_index_destroy(self._h)
@@ -221,6 +238,53 @@ class Index:
         cnt = c_uint64()
         check(load().fknn_filter_rows(self._h, m.ctypes.data, out.ctypes.data, byref(cnt), None))
         return out[: cnt.value].copy()
+
+
+def read_base_file(path: str):
+    """fknn_read_base_file (utils.h:257 ReadBase): (vecs (n,100), labels (n,), ts (n,)) float32."""
+    lib = load()
+    n = c_uint64()
+    check(lib.fknn_read_base_file(path.encode(), byref(n), None, None, None))
+    vecs = np.empty((n.value, DIM), np.float32)
+    labels = np.empty(n.value, np.float32)
+    ts = np.empty(n.value, np.float32)
+    check(lib.fknn_read_base_file(path.encode(), byref(n), vecs.ctypes.data, labels.ctypes.data, ts.ctypes.data))
+    return vecs, labels, ts
+
+
+def read_query_file(path: str):
+    """fknn_read_query_file (utils.h:550 ReadQuery): (qvecs (nq,100), metas (nq,4)) float32."""
+    lib = load()
+    nq = c_uint32()
+    check(lib.fknn_read_query_file(path.encode(), byref(nq), None, None))
+    q = np.empty((nq.value, DIM), np.float32)
+    m = np.empty((nq.value, 4), np.float32)
+    check(lib.fknn_read_query_file(path.encode(), byref(nq), q.ctypes.data, m.ctypes.data))
+    return q, m
+
+
+def sorted_query_order(metas) -> np.ndarray:
+    """fknn_sorted_query_order: the query order of ReadSortedQuery (utils.h:513-533)."""
+    m = np.ascontiguousarray(metas, dtype=np.float32).reshape(-1, 4)
+    out = np.empty(m.shape[0], np.uint32)
+    check(load().fknn_sorted_query_order(m.ctypes.data, m.shape[0], out.ctypes.data))
+    return out
+
+
+def save_knn(path: str, ids) -> None:
+    """fknn_save_knn (io.h:22 SaveKNN): nq x k uint32, no header."""
+    a = np.ascontiguousarray(ids, dtype=np.uint32)
+    check(load().fknn_save_knn(path.encode(), a.ctypes.data, a.shape[0], a.shape[1]))
+
+
+def read_groundtruth(path: str, k: int = K) -> np.ndarray:
+    """fknn_read_groundtruth (utils.h:194 ReadGroundTruth): (nq, k) uint32."""
+    lib = load()
+    nq = c_uint32()
+    check(lib.fknn_read_groundtruth(path.encode(), k, byref(nq), None))
+    out = np.empty((nq.value, k), np.uint32)
+    check(lib.fknn_read_groundtruth(path.encode(), k, byref(nq), out.ctypes.data))
+    return out
 
 
 def Bruteforce(nodes, queries, gt: Optional[list] = None):
