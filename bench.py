@@ -85,6 +85,9 @@ def parse():
     ap.add_argument("--graph", action="store_true",
                     help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
                          "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
+    ap.add_argument("--router", action="store_true",
+                    help="reference-routing run instead of the headline: fknn_router beside the reference pipeline's "
+                         "BatchSearch over the same subgraphs; q/s and recall per query type")
     ap.add_argument("--graph-beams", default="64,128,256,512")
     ap.add_argument("--graph-cats", type=int, default=8, help="largest categories that get a graph")
     a = ap.parse_args()
@@ -499,6 +502,64 @@ def run_graph(args):
     idx.close()
 
 
+def run_router(args):
+    """HybridGraph::BatchSearch's routing on the GPU (fknn_router) beside the
+    reference pipeline itself (oracle/_ref, its BatchSearch on the host
+    cores), over the same subgraphs and base orders the reference built
+    (HNSW M=16, efConstruction 100) on the uneven-selectivity generator;
+    queries/s of each (the router's wall time per call, host arrays in and
+    out, as the reference's BatchSearch is timed) and recall@100 per query
+    type against the exact ids."""
+    import torch
+
+    import fknn
+    import oracle
+    from fknn import datagen
+    torch.cuda.set_device(0)
+    if oracle.ref_hybrid() is None:
+        print(json.dumps({"mode": "router", "unavailable": "reference pipeline (oracle/_ref/libref_hybrid.so) not built"}))
+        return
+    n = args.n or 1_200_000
+    nq = args.nq or 20_000
+    vecs, labels, ts, q, metas = datagen.make_workload(4, n=n, nq=nq)
+    d = tempfile.mkdtemp()
+    datagen.write_base(d + "/base.bin", vecs, labels, ts)
+    datagen.write_queries(d + "/queries.bin", q, metas)
+    t0 = time.perf_counter()
+    ref_ids, ref_s = oracle.ref_hybrid_run(d + "/base.bin", d + "/queries.bin", d, nq)
+    ref_total = time.perf_counter() - t0
+    h = oracle.read_hybrid_dir(d, n)
+    with fknn.Index(vecs, labels, ts) as idx:
+        gt, _ = idx.search(q, metas)
+    with fknn.Router(vecs, labels, ts, h["sorted_base_ids"], h["sorted_base_ids_by_full_time"], h["categories"],
+                     h["buckets"], h["maxc_size"], h["minc_size"]) as router:
+        for _ in range(args.warmup):
+            ids, st = router.search(q, metas)
+        ms = []
+        for _ in range(args.steps):
+            t1 = time.perf_counter()
+            ids, st = router.search(q, metas)
+            ms.append((time.perf_counter() - t1) * 1e3)
+    rec = {}
+    for t in range(4):
+        sm = metas[:, 0] == t
+        rec[str(t)] = {"queries": int(sm.sum()), "router": datagen.recall_matrix(ids[sm], gt[sm]),
+                       "reference": datagen.recall_matrix(ref_ids[sm], gt[sm])}
+    print(json.dumps({"mode": "router", "metric": "filtered queries/s, reference routing (BatchSearch)", "unit": UNIT,
+                      "value": nq / (statistics.median(ms) * 1e-3), "ms_per_batch_median": statistics.median(ms),
+                      "recall_at_100_by_type": rec,
+                      "recall_at_100_all": {"router": datagen.recall_matrix(ids, gt),
+                                            "reference": datagen.recall_matrix(ref_ids, gt)},
+                      "routes": st,
+                      "reference_cpu": {"value": nq / ref_s, "unit": UNIT, "cores": os.cpu_count(),
+                                        "kind": "reference", "batchsearch_s": ref_s,
+                                        "build_and_search_s": ref_total},
+                      "config": {"workload": "uneven-selectivity (config-4 generator)", "n": n, "nq": nq,
+                                 "graphs": "reference HNSW, M=16, efConstruction=100",
+                                 "categories_with_graphs": len(h["categories"]), "time_buckets": len(h["buckets"])}}),
+          flush=True)
+
+
 def filter_measure(idx, metas, labels, ts, warmup: int, reps: int, batches=(1, 8)) -> dict:
     """fknn_filter_rows_batch (predicate + compaction, device-side counts)
     over the resident columns, the workload's predicates taken P at a time
@@ -672,6 +733,8 @@ def main():
         return run_filter(args)
     if args.graph:
         return run_graph(args)
+    if args.router:
+        return run_router(args)
     if args.sweep:
         return run_sweep(args)
     if args.serve:

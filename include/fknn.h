@@ -300,6 +300,72 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
                       uint32_t refine, const float *bounds, const int32_t *id_bounds, int32_t *out_ids,
                       float *out_dists, void *stream);
 
+/* ---- Reference-equivalent routing of HybridGraph::BatchSearch ----
+ *
+ * The reference answers its batch through a planner (hybrid_graph.cpp:
+ * 147-503): per query the selectivity sel = matches / sel_rows picks a
+ * route -- an SQ8 brute force over the query's slab (sel < bf_thr, or type 3
+ * and sel < bf_thr3), the category's graph (types 1 and 3, SearchFilter /
+ * SearchCategoryRange with a pool growing with the category's size), the
+ * ten time-bucket graphs (type 0, SearchFilterSubTime on each), or the
+ * buckets a window overlaps (type 2, SplitInterval: FULL / MEDIUM graph
+ * searches, SMALL brute force) -- and every route ends in an FP32 re-rank
+ * to the top 100.  fknn_router runs the same routes with the same
+ * thresholds, pools and merge rules on the GPU, over the reference's own
+ * subgraphs (Graph::save bytes) and base orders, so its recall can be
+ * compared with the reference pipeline's; the exact and BF16 forms of
+ * fknn_search need none of it. */
+typedef struct fknn_router fknn_router;
+
+typedef struct fknn_router_subgraph {
+  int32_t key;             /* category value, or time bucket t (timestamps in [t/10, (t+1)/10]) */
+  uint32_t start, count;   /* its rows: positions start .. start+count-1 of its base order */
+  const void *graph_bytes; /* Graph::save bytes of its graph (graph.hpp:101-115) */
+  size_t nbytes;
+} fknn_router_subgraph;
+
+typedef struct fknn_router_desc {
+  const float *vecs, *labels, *ts;           /* n x 100, n, n host floats, original row order (ids) */
+  uint64_t n;
+  const uint32_t *sorted_base_ids;           /* n: category order (label, ts) -> id   (utils.h:395-425) */
+  const uint32_t *sorted_base_ids_by_full_time; /* n: timestamp order -> id            (utils.h:420-425) */
+  const fknn_router_subgraph *categories;    /* graphs of the categories with their own (hybrid_graph.cpp:52-75) */
+  uint32_t ncategories;
+  const fknn_router_subgraph *buckets;       /* time-bucket graphs, in the order type 0 visits them
+                                                (hybrid_graph.cpp:303) */
+  uint32_t nbuckets;
+  uint32_t maxc_size, minc_size;             /* largest / smallest category size (utils.h:375-385) */
+  int device;
+} fknn_router_desc;
+
+/* SearchParams (hybrid_graph.h:14-34) and HybridGraph's thresholds
+ * (hybrid_graph.h:70-77, baseline.cpp:77-78); fknn_router_default_params
+ * fills the reference's values. */
+typedef struct fknn_router_params {
+  uint32_t ef0_full, ef1min, ef1max, ef3min, ef3max;
+  uint32_t ef2_full_large, ef2_full_medium, ef2_full_small;
+  uint32_t ef2_medium_large, ef2_medium_medium, ef2_medium_small;
+  float bf_thr, bf_thr3;
+  uint32_t bf_refine_k;      /* SQ8 brute-force candidates (140) */
+  uint32_t graph_refine_k;   /* graph candidates and merged pool size (150) */
+  uint32_t sel_rows;         /* selectivity denominator: the reference's 10,000,000 (hybrid_graph.cpp:151) */
+} fknn_router_params;
+
+typedef struct fknn_router_stats {
+  uint32_t n_bruteforce, n_category, n_type0, n_type2;  /* queries per route */
+  uint32_t n_graph_calls, n_split_small, n_split_medium, n_split_full;
+  float ms_total;            /* wall time of the call */
+} fknn_router_stats;
+
+int fknn_router_default_params(fknn_router_params *p);
+int fknn_router_create(const fknn_router_desc *desc, fknn_router **out);
+/* qvecs nq x 100 and metas nq x 4 (type, v, l, r) host floats; ids nq x 100
+ * host, ascending by FP32 distance, UINT32_MAX where a route found fewer
+ * rows.  params NULL = the reference's.  stats may be NULL. */
+int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, uint32_t nq,
+                       const fknn_router_params *params, uint32_t *ids, fknn_router_stats *stats);
+int fknn_router_destroy(fknn_router *r);
+
 /* ---- Request loop (continuous batching over one resident index) ----
  *
  * No reference counterpart: the reference answers one offline batch

@@ -127,6 +127,79 @@ struct HybridGraph {
   }
 };
 
+// hybrid_graph.h:37-109 with the reference's own routing
+// (hybrid_graph.cpp:147-503) run by fknn_router: the caller fills the
+// members the reference's caller fills (baseline.cpp:66-78, after
+// ReadSortedBaseTimestamp / ReadSortedQuery) plus the Graph::save bytes of
+// each category and time-bucket graph, calls Prepare once with the base in
+// original order, then BatchSearch with the reference's arguments.
+struct RoutedHybridGraph {
+  std::vector<uint32_t> sorted_ids;                    // query order (ReadSortedQuery)
+  std::vector<uint32_t> sorted_base_ids;               // category order -> id
+  std::vector<uint32_t> sorted_base_ids_by_full_time;  // timestamp order -> id
+  std::vector<std::pair<int32_t, std::pair<uint32_t, uint32_t>>> category_map, timestamp_map;  // key -> (start, n)
+  std::vector<std::pair<int32_t, std::string>> category_graphs, timestamp_graphs;  // key -> Graph::save bytes
+  uint32_t maxc_size = 0, minc_size = 0;
+  fknn_router_params params{};
+  fknn_router *router = nullptr;
+
+  RoutedHybridGraph() { fknn_router_default_params(&params); }
+  RoutedHybridGraph(const RoutedHybridGraph &) = delete;
+  RoutedHybridGraph &operator=(const RoutedHybridGraph &) = delete;
+  ~RoutedHybridGraph() {
+    if (router) fknn_router_destroy(router);
+  }
+
+  void Prepare(const float *vecs, const float *labels, const float *timestamps, uint64_t nb, int device = 0) {
+    if (router) fknn_router_destroy(router);
+    router = nullptr;
+    std::vector<fknn_router_subgraph> cats, bks;
+    auto add = [](const std::vector<std::pair<int32_t, std::pair<uint32_t, uint32_t>>> &map,
+                  const std::vector<std::pair<int32_t, std::string>> &graphs, std::vector<fknn_router_subgraph> &out) {
+      for (const auto &kv : map)
+        for (const auto &g : graphs)
+          if (g.first == kv.first) {
+            fknn_router_subgraph sg{};
+            sg.key = kv.first;
+            sg.start = kv.second.first;
+            sg.count = kv.second.second;
+            sg.graph_bytes = g.second.data();
+            sg.nbytes = g.second.size();
+            out.push_back(sg);
+          }
+    };
+    add(category_map, category_graphs, cats);
+    add(timestamp_map, timestamp_graphs, bks);
+    fknn_router_desc d{};
+    d.vecs = vecs;
+    d.labels = labels;
+    d.ts = timestamps;
+    d.n = nb;
+    d.sorted_base_ids = sorted_base_ids.data();
+    d.sorted_base_ids_by_full_time = sorted_base_ids_by_full_time.data();
+    d.categories = cats.data();
+    d.ncategories = (uint32_t)cats.size();
+    d.buckets = bks.data();
+    d.nbuckets = (uint32_t)bks.size();
+    d.maxc_size = maxc_size;
+    d.minc_size = minc_size;
+    d.device = device;
+    check(fknn_router_create(&d, &router));
+  }
+
+  // vecs / metas in sorted_ids order, as the reference's BatchSearch gets them
+  template <class Params = int>
+  void BatchSearch(const float * /*base*/, const float * /*base_by_time*/, const float * /*base_by_full_time*/,
+                   const float *vecs, const float *metas, int nq, uint32_t *ids, const Params & = {}) {
+    if (!router) throw std::runtime_error("BatchSearch: Prepare was not called");
+    if ((size_t)nq > sorted_ids.size()) throw std::runtime_error("BatchSearch: sorted_ids shorter than nq");
+    std::vector<uint32_t> tmp((size_t)nq * 100);
+    check(fknn_router_search(router, vecs, metas, (uint32_t)nq, &params, tmp.data(), nullptr));
+    for (int i = 0; i < nq; ++i)
+      std::memcpy(ids + (size_t)sorted_ids[i] * 100, tmp.data() + (size_t)i * 100, 100 * sizeof(uint32_t));
+  }
+};
+
 }  // namespace fknn_compat
 
 #endif  // FKNN_COMPAT_HPP_

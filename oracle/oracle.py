@@ -273,3 +273,57 @@ def ref_graph_search(path: str, vecs, labels, ts, queries, mode: int, k: int, re
     if rc != 0:
         raise RuntimeError("ref_graph_search failed")
     return (ids, d) if with_dists else ids
+
+
+_rh = None
+
+
+def ref_hybrid() -> ctypes.CDLL | None:
+    """The reference's whole approximate pipeline (baseline.cpp around
+    hybrid_graph.cpp) compiled from its sources, or None."""
+    global _rh
+    REF_HYBRID_SO = os.path.join(HERE, "_ref", "libref_hybrid.so")
+    if _rh is None and os.path.exists(REF_HYBRID_SO):
+        L = ctypes.CDLL(REF_HYBRID_SO)
+        L.ref_hybrid_run.restype = c_int
+        L.ref_hybrid_run.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, c_int, c_int, c_void_p,
+                                     POINTER(c_double)]
+        _rh = L
+    return _rh
+
+
+def ref_hybrid_run(base_path: str, query_path: str, out_dir: str, nq: int, M: int = 16, efc: int = 100):
+    """Runs the reference pipeline on contest files; returns (ids (nq,100)
+    u32 in query order, BatchSearch seconds).  The subgraphs, base orders
+    and maps it used are left in out_dir (read_hybrid_dir)."""
+    L = ref_hybrid()
+    if L is None:
+        raise RuntimeError("oracle/_ref/libref_hybrid.so is not built")
+    ids = np.empty((nq, 100), dtype=np.uint32)
+    sec = c_double()
+    rc = L.ref_hybrid_run(base_path.encode(), query_path.encode(), out_dir.encode(), M, efc, ids.ctypes.data,
+                          ctypes.byref(sec))
+    if rc != 0:
+        raise RuntimeError("ref_hybrid_run failed")
+    return ids, sec.value
+
+
+def read_hybrid_dir(out_dir: str, n: int) -> dict:
+    """The inputs the reference pipeline's BatchSearch used, as ref_hybrid_run
+    wrote them: the base orders, the category and time-bucket subgraphs
+    (key, start, count, Graph::save bytes; buckets in the reference's
+    visiting order) and the category size extremes."""
+    o = np.fromfile(os.path.join(out_dir, "orders.bin"), dtype=np.uint32).reshape(3, n)
+    cats, bks, maxc, minc = [], [], 0, 0
+    for line in open(os.path.join(out_dir, "maps.txt")):
+        f = line.split()
+        if f[0] == "c":
+            p = os.path.join(out_dir, f"c{f[1]}.hnsw")
+            if os.path.exists(p):  # categories without a graph have no file
+                cats.append((int(f[1]), int(f[2]), int(f[3]), open(p, "rb").read()))
+        elif f[0] == "t":
+            bks.append((int(f[1]), int(f[2]), int(f[3]), open(os.path.join(out_dir, f"t{f[1]}.hnsw"), "rb").read()))
+        elif f[0] == "m":
+            maxc, minc = int(f[2]), int(f[3])
+    return {"sorted_base_ids": o[0], "sorted_base_ids_by_time": o[1], "sorted_base_ids_by_full_time": o[2],
+            "categories": cats, "buckets": bks, "maxc_size": maxc, "minc_size": minc}

@@ -10,6 +10,11 @@
 //                 (distance.h:62-72).  Scalar code, built for baseline x86-64
 //                 plus AVX2/FMA exactly as the reference's CMakeLists.txt:14
 //                 asks, so it runs on any AVX2 host.
+//   * REF_HYBRID: the reference's whole approximate pipeline (baseline.cpp:
+//                 ReadSortedBaseTimestamp, ReadSortedQuery, HybridGraph::Build*,
+//                 the searchers, SortDataset and BatchSearch), with the graphs
+//                 and base orders it used written out so the GPU router can be
+//                 run on exactly the same inputs.
 //   * REF_SQ8   : bruteforce / bruteforce_subgraph (bruteforce.h:244-289),
 //                 L2SqrSQ8_sym (pyglass/glass/simd/distance.hpp:329-366) and
 //                 SQ8SymmetricQuantizer (pyglass/glass/quant/sq8_sym_quant.hpp).
@@ -144,6 +149,118 @@ int ref_graph_search(const char *path, const float *data, const float *labels, c
       default: return -1;
     }
   }
+  return 0;
+}
+}
+#endif
+
+#ifdef REF_HYBRID
+#include <fstream>
+#include <string>
+
+#include "hybrid_graph.cpp"
+
+extern "C" {
+// baseline.cpp:45-147 as a function over the contest files at base_path and
+// query_path, with BuildParams (M, efConstruction) given.  Before the
+// sub-graphs move into their searchers they are saved in Graph::save's
+// format to out_dir/c<category>.hnsw and out_dir/t<bucket>.hnsw; the three
+// base orders go to out_dir/orders.bin (3 x N u32: sorted_base_ids,
+// _by_time, _by_full_time) and the maps to out_dir/maps.txt ("c v start n",
+// "t t start n", "m maxc_id max_count min_count").  ids: nq x 100 u32 as
+// BatchSearch writes them; *seconds: the BatchSearch call alone.
+int ref_hybrid_run(const char *base_path, const char *query_path, const char *out_dir, int M, int efc,
+                   uint32_t *ids_out, double *seconds) {
+  std::vector<float> base_vecs, base_vecs_by_time, base_vecs_by_full_time;
+  std::vector<float> base_labels, base_labels_by_time, base_labels_by_full_time, base_timestamps,
+      base_timestamps_by_time, base_timestamps_by_full_time;
+  std::vector<float> query_vecs, query_metas;
+  std::vector<uint32_t> sorted_ids;
+  std::vector<uint32_t> sorted_base_ids, sorted_base_ids_by_time, sorted_base_ids_by_full_time;
+  std::unordered_map<int32_t, std::pair<uint32_t, uint32_t>> category_map, timestamp_map;
+  std::unordered_map<int32_t, std::vector<int>> category_query;
+  uint32_t nb, nq;
+  int maxc_id;
+  int32_t max_count = 0, min_count = 1e9;
+  ReadSortedBaseTimestamp(base_path, nb, base_vecs, base_labels, base_timestamps, sorted_base_ids, category_map,
+                          base_vecs_by_time, base_labels_by_time, base_timestamps_by_time, sorted_base_ids_by_time,
+                          maxc_id, base_vecs_by_full_time, base_labels_by_full_time, base_timestamps_by_full_time,
+                          sorted_base_ids_by_full_time, timestamp_map, max_count, min_count);
+  ReadSortedQuery(query_path, nq, query_vecs, query_metas, sorted_ids, category_query, category_map);
+  const std::string dir(out_dir);
+  {
+    std::ofstream o(dir + "/orders.bin", std::ios::binary);
+    o.write((const char *)sorted_base_ids.data(), (size_t)nb * 4);
+    o.write((const char *)sorted_base_ids_by_time.data(), (size_t)nb * 4);
+    o.write((const char *)sorted_base_ids_by_full_time.data(), (size_t)nb * 4);
+    std::ofstream m(dir + "/maps.txt");
+    for (auto &[v, p] : category_map) m << "c " << v << " " << p.first << " " << p.second << "\n";
+    for (auto &[t, p] : timestamp_map) m << "t " << t << " " << p.first << " " << p.second << "\n";
+    m << "m " << maxc_id << " " << max_count << " " << min_count << "\n";
+  }
+  HybridGraph h_graph;
+  h_graph.sorted_ids = std::move(sorted_ids);
+  h_graph.sorted_base_ids = std::move(sorted_base_ids);
+  h_graph.category_map = std::move(category_map);
+  h_graph.sorted_base_ids_by_time = std::move(sorted_base_ids_by_time);
+  h_graph.bf_thr = 0.045;
+  h_graph.cat_graph_thr = h_graph.bf_thr;
+  h_graph.maxc_id = maxc_id;
+  h_graph.timestamp_map = std::move(timestamp_map);
+  h_graph.sorted_base_ids_by_full_time = std::move(sorted_base_ids_by_full_time);
+  h_graph.maxc_size = max_count;
+  h_graph.minc_size = min_count;
+  h_graph.category_query = std::move(category_query);
+  BuildParams build_params;
+  build_params.M = M;
+  build_params.efConstruction = efc;
+  h_graph.Build(base_vecs_by_time.data(), base_labels_by_time.data(), base_timestamps_by_time.data(), nb,
+                build_params);
+  h_graph.BuildCategoryIndex(base_vecs.data(), base_labels.data(), base_timestamps.data(), nb, build_params);
+  h_graph.BuildTimestampIndex(base_vecs_by_full_time.data(), base_labels_by_full_time.data(),
+                              base_timestamps_by_full_time.data(), nb, build_params);
+  const uint32_t dim = h_graph.dim;
+  glass::Graph<int> graph;
+  h_graph.searcher = std::unique_ptr<glass::SearcherBase>(glass::create_searcher(std::move(graph), h_graph.metric, 3));
+  h_graph.searcher->SetData(base_vecs_by_time.data(), base_labels_by_time.data(), base_timestamps_by_time.data(), nb,
+                            dim);
+  std::vector<int> categories;
+  for (auto &[category, p] : h_graph.category_map)
+    if (p.second >= h_graph.cat_graph_thr * nb) categories.push_back(category);
+  for (int v : categories) {
+    auto &c_index = h_graph.category_index[v];
+    auto &fg = ((glass::HNSW *)c_index.get())->final_graph;
+    fg.save(dir + "/c" + std::to_string(v) + ".hnsw");
+    h_graph.category_searcher[v] =
+        std::unique_ptr<glass::SearcherBase>(glass::create_searcher(std::move(fg), h_graph.metric, 3));
+    auto &[start_id, n] = h_graph.category_map[v];
+    h_graph.category_searcher[v]->SetData(base_vecs.data() + (size_t)start_id * dim, base_labels.data() + start_id,
+                                          base_timestamps.data() + start_id, n, dim);
+  }
+  std::vector<int> buckets;
+  for (auto &[t, p] : h_graph.timestamp_map)
+    if (p.second) buckets.push_back(t);
+  for (int t : buckets) {
+    auto &t_index = h_graph.timestamp_index[t];
+    auto &fg = ((glass::HNSW *)t_index.get())->final_graph;
+    fg.save(dir + "/t" + std::to_string(t) + ".hnsw");
+    h_graph.timestamp_searcher[t] =
+        std::unique_ptr<glass::SearcherBase>(glass::create_searcher(std::move(fg), h_graph.metric, 3));
+    auto &[start_id, n] = h_graph.timestamp_map[t];
+    h_graph.timestamp_searcher[t]->SetData(base_vecs_by_full_time.data() + (size_t)start_id * dim,
+                                           base_labels_by_full_time.data() + start_id,
+                                           base_timestamps_by_full_time.data() + start_id, n, dim);
+  }
+  auto &quant = ((glass::Searcher<glass::SQ8SymmetricQuantizer<glass::Metric::L2>> *)h_graph.searcher.get())->quant;
+  h_graph.SortDataset(quant, base_labels_by_time.data(), base_timestamps_by_time.data(), nb);
+  SearchParams search_params;
+  std::vector<uint32_t> ids((size_t)nq * 100);
+  auto t0 = std::chrono::steady_clock::now();
+  h_graph.BatchSearch(base_vecs.data(), base_vecs_by_time.data(), base_vecs_by_full_time.data(), query_vecs.data(),
+                      query_metas.data(), nq, ids.data(), search_params);
+  auto t1 = std::chrono::steady_clock::now();
+  if (seconds) *seconds = std::chrono::duration<double>(t1 - t0).count();
+  std::memcpy(ids_out, ids.data(), ids.size() * 4);
   return 0;
 }
 }

@@ -283,6 +283,13 @@ int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t 
 int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
                 uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 
+// FP32 re-rank of device candidate lists, no synchronisation (rerank.cu)
+int launch_rerank(fknn_index *idx, const float *d_q, uint32_t nq, const uint32_t *d_cand, uint32_t nc, uint32_t k,
+                  uint32_t *d_ids, float *d_dists, int *d_err, cudaStream_t st);
+
+// a graph's device SQ8 codes (n x 112, its own points' order) and alpha (graph_search.cu)
+int graph_codes(const fknn_graph *g, const int8_t **codes, float *alpha, uint32_t *n);
+
 // symmetric SQ8 encoding of n x 100 device rows with a given alpha (sq8.cu)
 void launch_sq8_encode(const float *d_x, uint64_t n, float alpha, int8_t *d_codes, cudaStream_t st);
 

@@ -491,6 +491,17 @@ __global__ void __launch_bounds__(GS_WARPS * 32) k_graph_search(GParams P) {
   }
 }
 
+}  // namespace
+
+int graph_codes(const fknn_graph *g, const int8_t **codes, float *alpha, uint32_t *n) {
+  *codes = g->codes;
+  *alpha = g->alpha;
+  *n = g->n;
+  return FKNN_OK;
+}
+
+namespace {
+
 template <typename T>
 int grow(T **p, size_t *cap, size_t want) {
   if (*cap >= want) return FKNN_OK;

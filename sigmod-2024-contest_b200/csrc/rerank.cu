@@ -70,6 +70,20 @@ bool dev_ptr(const void *p) {
 }
 
 }  // namespace
+
+int launch_rerank(fknn_index *idx, const float *d_q, uint32_t nq, const uint32_t *d_cand, uint32_t nc, uint32_t k,
+                  uint32_t *d_ids, float *d_dists, int *d_err, cudaStream_t st) {
+  if (nq == 0) return FKNN_OK;
+  if (nc == 0 || nc > (uint32_t)RK_MAXC || k == 0 || k > nc) {
+    set_error("re-rank: need 1 <= k <= nc <= 2048");
+    return FKNN_EINVAL;
+  }
+  k_rerank<<<nq, RK_THREADS, 0, st>>>(idx->vecs, idx->n, d_q, nq, d_cand, nc, k, d_ids, d_dists, d_err);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
 }  // namespace fknn
 
 using namespace fknn;

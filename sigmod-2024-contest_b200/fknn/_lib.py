@@ -116,6 +116,35 @@ class ServerStats(Structure):
         return {f: getattr(self, f) for f, _ in self._fields_}
 
 
+class RouterSubgraph(Structure):
+    _fields_ = [("key", ctypes.c_int32), ("start", c_uint32), ("count", c_uint32), ("graph_bytes", c_void_p),
+                ("nbytes", c_size_t)]
+
+
+class RouterDesc(Structure):
+    _fields_ = [("vecs", c_void_p), ("labels", c_void_p), ("ts", c_void_p), ("n", c_uint64),
+                ("sorted_base_ids", c_void_p), ("sorted_base_ids_by_full_time", c_void_p),
+                ("categories", POINTER(RouterSubgraph)), ("ncategories", c_uint32),
+                ("buckets", POINTER(RouterSubgraph)), ("nbuckets", c_uint32), ("maxc_size", c_uint32),
+                ("minc_size", c_uint32), ("device", c_int)]
+
+
+class RouterParams(Structure):
+    _fields_ = [(f, c_uint32) for f in ("ef0_full", "ef1min", "ef1max", "ef3min", "ef3max", "ef2_full_large",
+                                        "ef2_full_medium", "ef2_full_small", "ef2_medium_large",
+                                        "ef2_medium_medium", "ef2_medium_small")] + \
+               [("bf_thr", c_float), ("bf_thr3", c_float), ("bf_refine_k", c_uint32), ("graph_refine_k", c_uint32),
+                ("sel_rows", c_uint32)]
+
+
+class RouterStats(Structure):
+    _fields_ = [(f, c_uint32) for f in ("n_bruteforce", "n_category", "n_type0", "n_type2", "n_graph_calls",
+                                        "n_split_small", "n_split_medium", "n_split_full")] + [("ms_total", c_float)]
+
+    def as_dict(self) -> dict:
+        return {f: getattr(self, f) for f, _ in self._fields_}
+
+
 # Every entry point of include/fknn.h with its ctypes signature.
 SIGNATURES = {
     "fknn_version": (c_int, []),
@@ -155,6 +184,11 @@ SIGNATURES = {
     "fknn_graph_info": (c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_float)]),
     "fknn_graph_search": (c_int, [c_void_p, c_void_p, c_uint32, c_int, c_uint32, c_uint32, c_uint32, c_void_p,
                                   c_void_p, c_void_p, c_void_p, c_void_p]),
+    "fknn_router_default_params": (c_int, [POINTER(RouterParams)]),
+    "fknn_router_create": (c_int, [POINTER(RouterDesc), POINTER(c_void_p)]),
+    "fknn_router_search": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, POINTER(RouterParams), c_void_p,
+                                   POINTER(RouterStats)]),
+    "fknn_router_destroy": (c_int, [c_void_p]),
     "fknn_server_create": (c_int, [c_void_p, POINTER(ServerOpts), POINTER(c_void_p)]),
     "fknn_server_now_ns": (ctypes.c_int64, []),
     "fknn_server_submit": (c_int, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p, c_void_p, c_void_p,

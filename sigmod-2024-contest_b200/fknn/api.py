@@ -240,6 +240,70 @@ class Index:
         return out[: cnt.value].copy()
 
 
+class Router:
+    """fknn_router: HybridGraph::BatchSearch's routing (hybrid_graph.cpp:
+    147-503) on the GPU, over the reference's subgraphs and base orders.
+
+    categories / buckets: lists of (key, start, count, Graph::save bytes);
+    buckets in the order the reference visits them for type-0 queries."""
+
+    def __init__(self, vecs, labels, ts, sorted_base_ids, sorted_base_ids_by_full_time, categories, buckets,
+                 maxc_size: int, minc_size: int, device: int = 0):
+        lib = load()
+        self._keep = [np.ascontiguousarray(vecs, np.float32), np.ascontiguousarray(labels, np.float32),
+                      np.ascontiguousarray(ts, np.float32), np.ascontiguousarray(sorted_base_ids, np.uint32),
+                      np.ascontiguousarray(sorted_base_ids_by_full_time, np.uint32)]
+        v, l, t, sb, sf = self._keep
+
+        def subs(lst):
+            arr = (_lib.RouterSubgraph * max(1, len(lst)))()
+            for i, (key, start, count, gb) in enumerate(lst):
+                buf = np.frombuffer(bytes(gb), dtype=np.uint8)
+                self._keep.append(buf)
+                arr[i] = _lib.RouterSubgraph(int(key), int(start), int(count), buf.ctypes.data, buf.size)
+            return arr
+        ca, ba = subs(categories), subs(buckets)
+        d = _lib.RouterDesc(v.ctypes.data, l.ctypes.data, t.ctypes.data, v.shape[0], sb.ctypes.data, sf.ctypes.data,
+                            ca, len(categories), ba, len(buckets), int(maxc_size), int(minc_size), device)
+        h = c_void_p()
+        check(lib.fknn_router_create(byref(d), byref(h)))
+        self._h = h
+        self._keep = None  # the router holds its own copies
+
+    @staticmethod
+    def default_params() -> "_lib.RouterParams":
+        p = _lib.RouterParams()
+        check(load().fknn_router_default_params(byref(p)))
+        return p
+
+    def search(self, qvecs, metas, params=None):
+        """ids (nq, 100) uint32 and the per-route statistics."""
+        q = np.ascontiguousarray(qvecs, np.float32)
+        m = np.ascontiguousarray(metas, np.float32)
+        ids = np.empty((q.shape[0], K), np.uint32)
+        st = _lib.RouterStats()
+        check(load().fknn_router_search(self._h, q.ctypes.data, m.ctypes.data, q.shape[0],
+                                        byref(params) if params is not None else None, ids.ctypes.data, byref(st)))
+        return ids, st.as_dict()
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            load().fknn_router_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
 def read_base_file(path: str):
     """fknn_read_base_file (utils.h:257 ReadBase): (vecs (n,100), labels (n,), ts (n,)) float32."""
     lib = load()
