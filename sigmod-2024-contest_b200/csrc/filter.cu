@@ -5,12 +5,12 @@
 //
 // Two launches, and the columns are read once for up to FP_MAXP predicates:
 //   k_filter_mark  each CTA owns one contiguous, equal row range; per
-//                  4,096-row chunk every thread loads 16 labels and 16
+//                  2,048-row chunk every thread loads 8 labels and 8
 //                  timestamps (coalesced), and every predicate's warp ballots
 //                  are stored as a bit per row (N/8 bytes per predicate,
 //                  which stays in L2) plus the CTA's passing count;
 //   k_filter_emit  per (CTA range, predicate): the sum of the counts of the
-//                  ranges before it, then per chunk a scan of the 128 words'
+//                  ranges before it, then per chunk a scan of the 64 words'
 //                  popcounts, and every passing row writes its id at
 //                  base + word offset + its rank inside the word.
 // Nothing is read back: the counts land in device memory, so a batch of
@@ -27,12 +27,12 @@ namespace fknn {
 namespace {
 
 constexpr int FP_THREADS = 256;
-constexpr int FP_ITEMS = 16;
+constexpr int FP_ITEMS = 8;
 constexpr int FP_CHUNK = FP_THREADS * FP_ITEMS;  // rows per chunk
 constexpr int FP_WORDS = FP_CHUNK / 32;          // bit words per chunk
 constexpr int FP_NW = FP_THREADS / 32;
 constexpr uint32_t FP_MAXP = 16;                 // predicates per launch
-constexpr int FP_CTAS_PER_SM = 4;                // resident at <= 64 registers: one wave
+constexpr int FP_CTAS_PER_SM = 8;                // resident at <= 32 registers: one wave
 
 struct FilterPreds {
   float4 m[FP_MAXP];  // (type, v, l, r), checked on the host
@@ -55,8 +55,10 @@ __global__ void __launch_bounds__(FP_THREADS, FP_CTAS_PER_SM) k_filter_mark(cons
                                                             uint32_t *__restrict__ bits, uint64_t words_per_pred,
                                                             uint32_t *__restrict__ cta_cnt) {
   __shared__ uint32_t wcnt[FP_MAXP][FP_NW];
+  __shared__ float4 pm[FP_MAXP];  // the predicates, indexed at run time (kept out of local memory)
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   for (int i = tid; i < (int)(FP_MAXP * FP_NW); i += FP_THREADS) (&wcnt[0][0])[i] = 0;
+  if (tid < (int)FP_MAXP) pm[tid] = P.m[tid];
   __syncthreads();
   const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_cta;
   const uint64_t r1 = min(n, r0 + rows_per_cta);
@@ -74,7 +76,7 @@ __global__ void __launch_bounds__(FP_THREADS, FP_CTAS_PER_SM) k_filter_mark(cons
       }
     }
     for (uint32_t p = 0; p < np; ++p) {
-      const float4 m = P.m[p];
+      const float4 m = pm[p];
       uint32_t mine = 0, cnt = 0;
 #pragma unroll
       for (int i = 0; i < FP_ITEMS; ++i) {
@@ -131,7 +133,7 @@ __global__ void __launch_bounds__(FP_THREADS) k_filter_emit(uint64_t n, uint64_t
   uint32_t *op = out + (uint64_t)p * out_stride;
   const uint32_t lt = (1u << lane) - 1u;
   for (uint64_t c0 = r0; c0 < r1; c0 += FP_CHUNK) {
-    // exclusive scan of the chunk's 128 word popcounts (warps 0-3)
+    // exclusive scan of the chunk's FP_WORDS word popcounts
     if (tid < FP_WORDS) {
       const uint32_t word = (c0 + (uint64_t)tid * 32 < r1) ? __ldcs(bp + c0 / 32 + tid) : 0u;
       const uint32_t pc = __popc(word);

@@ -409,9 +409,9 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
   fknn_router_params P;
   if (params) P = *params;
   else fknn_router_default_params(&P);
-  if (P.bf_refine_k == 0 || P.bf_refine_k > (uint32_t)ST_KMAX || P.graph_refine_k < 100 ||
+  if (P.bf_refine_k < 100 || P.bf_refine_k > (uint32_t)ST_KMAX || P.graph_refine_k < 100 ||
       P.graph_refine_k > 2048 || P.sel_rows == 0) {
-    set_error("fknn_router_search: need 1 <= bf_refine_k <= 256, 100 <= graph_refine_k <= 2048, sel_rows > 0");
+    set_error("fknn_router_search: need 100 <= bf_refine_k <= 256, 100 <= graph_refine_k <= 2048, sel_rows > 0");
     return FKNN_EINVAL;
   }
   if (nq == 0) return FKNN_OK;

@@ -33,7 +33,7 @@ def test_config1_whole():
     assert (ids == UMAX).any()
 
 
-def pick_queries(counts, types, rng, n_random=192):
+def pick_queries(counts, types, rng, n_random=256):
     """Indices of a checked sample: the 32 largest slabs, up to 32 queries
     with fewer than 100 passing rows (or the smallest slabs), and a random
     draw of n_random stratified by query type."""

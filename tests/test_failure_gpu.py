@@ -37,7 +37,7 @@ def test_device_wait_runs_out_then_next_call_succeeds(data):
     want, wd = idx.search(q, metas, mode=fknn.MODE_BF16_RERANK, kprime=200)
     exact, ed = idx.search(q, metas, mode=fknn.MODE_EXACT_FP32)
     assert lib.fknn_index_test_withhold_copy(idx._h) == fknn.FKNN_OK
-    ids = np.full_like(want, 7)
+    ids = np.full_like(want, 0xFFFFFFFE)  # neither a row id nor the padding value
     dd = np.zeros_like(wd)
     t0 = time.perf_counter()
     with pytest.raises(fknn.FknnError) as e:
@@ -53,7 +53,7 @@ def test_device_wait_runs_out_then_next_call_succeeds(data):
     same = np.all(ids == want, axis=1)
     exact_rows = np.all(ids == exact, axis=1)
     assert (~(same | exact_rows)).sum() <= q.shape[0] // 100
-    assert (ids != 7).all() and np.isfinite(dd[ids != 0xFFFFFFFF]).all()
+    assert (ids != 0xFFFFFFFE).all() and np.isfinite(dd[ids != 0xFFFFFFFF]).all()
     # the hook is off again and the context is healthy
     again, ad = idx.search(q, metas, mode=fknn.MODE_BF16_RERANK, kprime=200)
     assert (~np.all(again == want, axis=1)).sum() <= q.shape[0] // 100
