@@ -68,8 +68,9 @@ typedef struct fknn_tuning {
   uint32_t items_per_sm;     /* contraction work items per SM: load balance against candidate traffic */
   uint32_t min_chunk_blocks; /* shortest row chunk of a work item, in row blocks (64 rows exact, 128 BF16/FP8) */
   uint32_t bound_refresh;    /* BF16/FP8: sub-tiles between reloads of the shared per-query bound (0 = at trims) */
-  uint32_t pilot_stride;     /* BF16/FP8: a pilot pass over every pilot_stride-th row block first seeds the
-                                bound of long queries (0 or 1 = no pilot) */
+  uint32_t pilot_stride;     /* a pilot pass over every pilot_stride-th row block first seeds the bounds
+                                (0 or 1 = no pilot).  BF16/FP8: an estimate of the k'-th, checked by the
+                                merge; exact: the k-th of the sample, a valid upper bound */
 } fknn_tuning;
 
 typedef struct fknn_search_opts {

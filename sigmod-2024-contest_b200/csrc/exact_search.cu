@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
              const int32_t *__restrict__ lane_q, const uint32_t *__restrict__ lane_s,
              const uint32_t *__restrict__ lane_e, const float *__restrict__ blocks_t,
              const float *__restrict__ blocks_c, uint32_t *__restrict__ T_global, uint32_t *__restrict__ ovf,
-             Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt, uint32_t k, int *err) {
+             Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt, uint32_t k, uint32_t stride, int *err) {
   extern __shared__ __align__(128) unsigned char smem_raw[];
   ScreenSmem &sm = *reinterpret_cast<ScreenSmem *>(smem_raw);
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -271,7 +271,8 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
   const WorkItem it = items[item_id];
   const Tile tl = tiles[it.tile];
   const float *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
-  const uint32_t nsub = it.blk1 - it.blk0;
+  // every stride-th row block of the item (stride 1: all of them)
+  const uint32_t nsub = (it.blk1 - it.blk0 + stride - 1) / stride;
   Candidate *out_item = out + (uint64_t)item_id * TQ * CAP;
 
   if (tid == 0) {
@@ -294,7 +295,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
         const int st = sub % SC_STAGES;
         if (sub >= SC_STAGES && !mbar_wait_bounded(&sm.empty[st], ((sub / SC_STAGES) - 1) & 1, err)) break;
         mbar_arrive_expect_tx(&sm.full[st], BLK_BYTES);
-        bulk_g2s(sm.xs[st], blocks + (uint64_t)(it.blk0 + sub) * BLK_FLOATS, BLK_BYTES, &sm.full[st]);
+        bulk_g2s(sm.xs[st], blocks + (uint64_t)(it.blk0 + sub * stride) * BLK_FLOATS, BLK_BYTES, &sm.full[st]);
         ++issued;
       }
       // every issued copy must have landed before the CTA may exit
@@ -361,7 +362,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
     if (lane == 0) mbar_arrive(&sm.empty[st]);  // this warp is done with the slot
     // epilogue: ds = (|x|^2 + |q|^2) - 2 q.x; keep rows that can reach the bound
     const float xn[4] = {xn4.x, xn4.y, xn4.z, xn4.w};
-    const uint32_t row0 = (it.blk0 + sub) * BLK + ty * 4;
+    const uint32_t row0 = (it.blk0 + sub * stride) * BLK + ty * 4;
     uint32_t pass = 0;
 #pragma unroll
     for (int j = 0; j < 8; ++j) {
@@ -1196,10 +1197,27 @@ int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_
     FKNN_CUDA(cudaFuncSetAttribute(k_screen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     FKNN_CUDA(cudaFuncSetAttribute(k_merge, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(MergeSmem)));
     if (stats) FKNN_CUDA(cudaEventRecord(ev[0], st));
+    const uint32_t pstride = idx->tuning[FKNN_MODE_EXACT_FP32].pilot_stride;
+    if (pstride > 1) {
+      // Pilot: the same screen over every pstride-th row block.  Each list's
+      // k-th screening distance (widened by screen_hi) bounds the k-th
+      // reference distance of its query from above -- the k-th smallest of
+      // a subset is never below the k-th smallest of the whole slab -- so the
+      // bounds it leaves in T_global are valid seeds and the main pass keeps
+      // every row that can be in the top k.  Its overflow marks are its own.
+      uint32_t *ovf_p;
+      if ((rc = ws_get(idx, 13, (size_t)nq * 4, (void **)&ovf_p))) return rc;
+      FKNN_CUDA(cudaMemsetAsync(ovf_p, 0, (size_t)nq * 4, st));
+      k_screen<<<nitems, SC_THREADS, smem, st>>>(
+          (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_qt,
+          (const int32_t *)(d_blob + o_lq), (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le),
+          OT.blocks, OC.blocks, T_global, ovf_p, d_out, d_ocnt, k, pstride, idx->d_flag);
+      g_launches += 1;
+    }
     k_screen<<<nitems, SC_THREADS, smem, st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_qt, (const int32_t *)(d_blob + o_lq),
         (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), OT.blocks, OC.blocks, T_global, ovf,
-        d_out, d_ocnt, k, idx->d_flag);
+        d_out, d_ocnt, k, 1u, idx->d_flag);
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     k_merge<<<nbig, MG_THREADS, sizeof(MergeSmem), st>>>(
         (const uint32_t *)(d_blob + o_big), (const uint32_t *)(d_blob + o_btile), (const uint32_t *)(d_blob + o_blane),
