@@ -416,15 +416,17 @@ def run_serve(args):
 def run_graph(args):
     """Per-category graph search (config-4 generator, Zipf 1.5 over 10,000
     categories): one graph of out-degree 32 per large category, built by the
-    reference's HNSW::Build (oracle/_ref) over that category's rows; every
-    type-1 query of those categories searches its category's graph with
-    SearchFilter (pool = beam) on the GPU, its refine=min(150, beam)
+    reference's HNSW::Build (oracle/_ref) over that category's rows in
+    timestamp order (the order the reference's category searchers hold,
+    utils.h:395-425).  Type-1 queries of those categories search their
+    category's graph with SearchFilter and type-3 queries with
+    SearchCategoryRange (the window and its row range seed the pool,
+    searcher.hpp:301-374), pool = beam; their refine = min(150, beam)
     candidates are re-ranked in FP32 on the GPU (fknn_rerank), and recall@100
-    is taken against the exact path's ids.  queries/s counts the graph
-    search plus the re-rank, inputs resident.  The reference Searcher is
-    timed on a sample of the same queries on one host thread."""
-    import ctypes
-
+    is taken per type against the exact path's ids.  queries/s counts the
+    graph searches plus the re-ranks, inputs resident.  The reference
+    Searcher is timed on a sample of the largest category's type-1 queries
+    on one host thread."""
     import torch
 
     import fknn
@@ -446,16 +448,31 @@ def run_graph(args):
     tmp = tempfile.mkdtemp()
     for c in cats:
         rows = np.nonzero(lab == c)[0]
+        rows = rows[np.argsort(ts[rows], kind="stable")]
         t0 = time.perf_counter()
         gb = oracle.ref_hnsw_graph(vecs[rows], ts[rows], 32, 100, os.path.join(tmp, f"g{c}.bin"))
         t_build += time.perf_counter() - t0
         graphs[int(c)] = (rows, fknn.GraphSearcher(gb, vecs[rows]), os.path.join(tmp, f"g{c}.bin"))
-    sel = np.nonzero((metas[:, 0] == 1) & np.isin(metas[:, 1].astype(np.int64), cats))[0]
+    catq = np.isin(metas[:, 1].astype(np.int64), cats)
+    sel = np.nonzero(((metas[:, 0] == 1) | (metas[:, 0] == 3)) & catq)[0]
     qs, ms = q[sel], metas[sel]
     exact_ids, _ = idx.search(qs, ms, k=100, mode=fknn.MODE_EXACT_FP32)
-    per_cat = {int(c): np.nonzero(ms[:, 1].astype(np.int64) == c)[0] for c in cats}
-    dq = {c: torch.from_numpy(np.ascontiguousarray(qs[ix])).cuda() for c, ix in per_cat.items()}
-    rows_t = {c: torch.from_numpy(graphs[c][0].astype(np.int64)).cuda() for c in per_cat}
+    groups = {}
+    for c in cats:
+        for t in (1, 3):
+            ix = np.nonzero((ms[:, 1].astype(np.int64) == c) & (ms[:, 0] == t))[0]
+            if len(ix) == 0:
+                continue
+            rows = graphs[int(c)][0]
+            tr = ts[rows]
+            g = {"ix": ix, "q": torch.from_numpy(np.ascontiguousarray(qs[ix])).cuda(),
+                 "rows": torch.from_numpy(rows.astype(np.int64)).cuda()}
+            if t == 3:
+                l, r = ms[ix, 2], ms[ix, 3]
+                g["bounds"] = np.ascontiguousarray(np.stack([l, r], 1), np.float32)
+                g["id_bounds"] = np.ascontiguousarray(np.stack([np.searchsorted(tr, l, "left"),
+                                                                np.searchsorted(tr, r, "right")], 1), np.int32)
+            groups[(int(c), t)] = g
     for beam in [int(b) for b in args.graph_beams.split(",")]:
         refine = min(150, beam)
         out = np.full((len(sel), 100), 0xFFFFFFFF, np.uint32)  # beams under 100 return fewer ids
@@ -464,22 +481,22 @@ def run_graph(args):
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
             res = {}
-            for c, ix in per_cat.items():
-                if len(ix) == 0:
-                    continue
-                loc = graphs[c][1].SearchFilter(dq[c], beam, refine)
-                cand = rows_t[c][loc.long()].to(torch.int32).contiguous()
-                res[c] = idx.rerank(dq[c], cand, k=min(100, refine), with_dists=False)[0]
+            for (c, t), g in groups.items():
+                gs = graphs[c][1]
+                if t == 1:
+                    loc = gs.SearchFilter(g["q"], beam, refine)
+                else:
+                    loc = gs.SearchCategoryRange(g["q"], beam, refine, g["bounds"], g["id_bounds"])
+                cand = g["rows"][loc.long().clamp(min=0)].to(torch.int32).contiguous()
+                res[(c, t)] = idx.rerank(g["q"], cand, k=min(100, refine), with_dists=False)[0]
             e1.record()
             torch.cuda.synchronize()
         ms_gpu = e0.elapsed_time(e1)
-        for c, ix in per_cat.items():
-            if c in res:
-                out[ix, :res[c].shape[1]] = res[c].cpu().numpy().view(np.uint32)
-        rec = datagen.recall_matrix(out, exact_ids)
-        # reference Searcher (mode 1 = SearchFilter) on a sample of the top category's queries, one thread
+        for key, g in groups.items():
+            out[g["ix"], :res[key].shape[1]] = res[key].cpu().numpy().view(np.uint32)
+        rec = {str(t): datagen.recall_matrix(out[ms[:, 0] == t], exact_ids[ms[:, 0] == t]) for t in (1, 3)}
         c0 = int(cats[0])
-        smp = per_cat[c0][:min(len(per_cat[c0]), 300)]
+        smp = groups[(c0, 1)]["ix"][:300]
         rows0 = graphs[c0][0]
         v0, l0, t0_ = vecs[rows0], labels[rows0], ts[rows0]
         t0 = time.perf_counter()  # graph load + SetData's quantizer training, subtracted below
@@ -491,13 +508,15 @@ def run_graph(args):
         print(json.dumps({
             "mode": "graph", "metric": "filtered queries/s, graph beam search + FP32 re-rank", "unit": UNIT,
             "value": len(sel) / (ms_gpu * 1e-3), "ms": ms_gpu, "beam": beam, "refine": refine,
-            "recall_at_100_vs_exact": rec,
+            "recall_at_100_vs_exact": datagen.recall_matrix(out, exact_ids), "recall_at_100_by_type": rec,
             "config": {"workload": "uneven-selectivity (config-4 generator)", "n": n, "queries": int(len(sel)),
-                       "query_type": 1, "categories_with_graphs": [int(c) for c in cats],
+                       "query_types": {"1": int((ms[:, 0] == 1).sum()), "3": int((ms[:, 0] == 3).sum())},
+                       "categories_with_graphs": [int(c) for c in cats],
                        "category_rows": [int(counts[c]) for c in cats], "out_degree": 32, "ef_construction": 100},
             "graph_build_s_reference_cpu": t_build,
             "reference_cpu": {"value": len(smp) / t_ref, "unit": UNIT, "cores": 1, "kind": "reference",
-                              "sample": f"{len(smp)} queries of category {c0} (largest graph), SearchFilter, one thread"},
+                              "sample": f"{len(smp)} type-1 queries of category {c0} (largest graph), SearchFilter, "
+                                        f"one thread"},
         }), flush=True)
     idx.close()
 

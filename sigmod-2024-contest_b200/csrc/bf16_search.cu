@@ -80,6 +80,26 @@ __device__ __forceinline__ void umma(uint32_t tmem_d, uint64_t da, uint64_t db, 
   }
 }
 
+// max of 32 values as a tree of three-input maxima (16 instructions)
+__device__ __forceinline__ float max32(const float *v) {
+  float a[10];
+#pragma unroll
+  for (int k = 0; k < 10; ++k) a[k] = fmax3(v[3 * k], v[3 * k + 1], v[3 * k + 2]);
+  const float b0 = fmax3(a[0], a[1], a[2]), b1 = fmax3(a[3], a[4], a[5]), b2 = fmax3(a[6], a[7], a[8]);
+  const float b3 = fmax3(a[9], v[30], v[31]);
+  return fmax3(b0, b1, fmaxf(b2, b3));
+}
+
+// bit j set iff v[j] >= t, built as four independent chains
+__device__ __forceinline__ uint32_t ge_mask32(const float *v, float t) {
+  uint32_t p[4] = {0u, 0u, 0u, 0u};
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
+#pragma unroll
+    for (int g = 0; g < 4; ++g) p[g] |= (v[g * 8 + j] >= t ? 1u : 0u) << (g * 8 + j);
+  return (p[0] | p[1]) | (p[2] | p[3]);
+}
+
 // ------------------------------------------------------------- build ---
 
 __global__ void k_build_bf16_blocks(const float *__restrict__ vecs, const float *__restrict__ norms,
@@ -267,11 +287,9 @@ static_assert(sizeof(BScreenSmem<FmtBF16>) <= 113 * 1024 && sizeof(BScreenSmem<F
 
 // Screens 32 accumulator columns c .. c+31 of one query (this lane): every
 // column j inside the slab [r0, r1) with acc >= cq is appended to the
-// query's list with its screening distance qn - 2 sc acc.  The columns are
-// reduced as eleven groups (ten triples and a pair) by three-input maxima;
-// only when the chunk's maximum reaches cq are the values staged in the
-// lane's shared-memory row and the groups whose maximum reaches it
-// searched, so a chunk with one candidate costs a few dozen instructions.
+// query's list with its screening distance qn - 2 sc acc.  The lane's
+// candidates form a bit mask; their values are read back from the lane's
+// shared-memory staging row, so the push loop runs once per candidate.
 __device__ __forceinline__ int screen_chunk(const uint32_t (&r)[32], int c, int r0, int r1, float cq, float qn,
                                             float sc, uint32_t p0, float *row, Candidate *list, int cnt) {
   if (r0 >= c + 32 || r1 <= c) return cnt;
@@ -283,31 +301,18 @@ __device__ __forceinline__ int screen_chunk(const uint32_t (&r)[32], int c, int 
     for (int j = 0; j < 32; ++j)
       if (c + j < r0 || c + j >= r1) v[j] = -INFINITY;
   }
-  float g[11];
-#pragma unroll
-  for (int k = 0; k < 10; ++k) g[k] = fmax3(v[3 * k], v[3 * k + 1], v[3 * k + 2]);
-  g[10] = fmaxf(v[30], v[31]);
-  const float m = fmax3(fmax3(g[0], g[1], g[2]), fmax3(g[3], g[4], g[5]), fmax3(fmax3(g[6], g[7], g[8]), g[9], g[10]));
-  if (m >= cq) {
+  if (max32(v) >= cq) {
+    uint32_t mask = ge_mask32(v, cq);
 #pragma unroll
     for (int j = 0; j < 32; j += 4)
       *reinterpret_cast<float4 *>(row + j) = make_float4(v[j], v[j + 1], v[j + 2], v[j + 3]);
-    uint32_t gm = 0;
-#pragma unroll
-    for (int k = 0; k < 11; ++k) gm |= (g[k] >= cq ? 1u : 0u) << k;
-    while (gm) {
-      const int k = __ffs(gm) - 1;
-      gm &= gm - 1;
-      const int j0 = 3 * k, jn = k == 10 ? 2 : 3;
-      for (int t = 0; t < jn; ++t) {
-        const float x = row[j0 + t];
-        if (x >= cq) {
-          Candidate cd;
-          cd.ds = fmaf(-2.f * sc, x, qn);
-          cd.pos = p0 + c + j0 + t;
-          list[cnt++] = cd;
-        }
-      }
+    while (mask) {
+      const int j = __ffs(mask) - 1;
+      mask &= mask - 1;
+      Candidate cd;
+      cd.ds = fmaf(-2.f * sc, row[j], qn);
+      cd.pos = p0 + c + j;
+      list[cnt++] = cd;
     }
   }
   return cnt;

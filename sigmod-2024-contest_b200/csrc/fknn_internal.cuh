@@ -215,7 +215,7 @@ struct fknn_index {
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   fknn::Plan plan;  // rebuilt by every search; capacity kept
   // per-mode plan / kernel parameters (fknn_index_set_tuning) and the SM count
-  fknn_tuning tuning[3] = {{0, 16, 16, 0, 16}, {256, 3, 8, 0, 16}, {256, 3, 8, 0, 16}};
+  fknn_tuning tuning[3] = {{0, 16, 16, 0, 0}, {256, 3, 8, 0, 16}, {256, 3, 8, 0, 16}};
   int num_sms = 148;
   // a view shares the device data of another index and owns only its
   // per-call scratch (ws, hs, d_flag), so views search concurrently
