@@ -184,7 +184,10 @@ int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, u
  * per pass, row p of out_ids (DEVICE memory, np x n uint32, row stride n)
  * receives predicate p's passing ids in increasing order and counts[p]
  * (DEVICE memory, np uint64) their number.  Nothing is read back; results
- * are complete when `stream` reaches the point of the call. */
+ * are complete when `stream` reaches the point of the call.  A count of
+ * UINT64_MAX means the kernel's bounded wait gave up (its ids are then
+ * incomplete); it does not happen in normal operation.  Calls on one index
+ * share its scratch: issue them on one stream. */
 int fknn_filter_rows_batch(fknn_index *index, const float *metas, uint32_t np, uint32_t *out_ids,
                            uint64_t *counts, void *stream);
 

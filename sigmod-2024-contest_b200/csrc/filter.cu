@@ -3,20 +3,24 @@
 // int32(v), 2 l <= ts <= r, 3 both) applied to whole columns, writing each
 // predicate's passing row ids in increasing order.
 //
-// Two launches, and the columns are read once for up to FP_MAXP predicates:
-//   k_filter_mark  each CTA owns one contiguous, equal row range; per
-//                  2,048-row chunk every thread loads 8 labels and 8
-//                  timestamps (coalesced), and every predicate's warp ballots
-//                  are stored as a bit per row (N/8 bytes per predicate,
-//                  which stays in L2) plus the CTA's passing count;
-//   k_filter_emit  per (CTA range, predicate): the sum of the counts of the
-//                  ranges before it, then per chunk a scan of the 64 words'
-//                  popcounts, and every passing row writes its id at
-//                  base + word offset + its rank inside the word.
+// One pass over the columns for up to FP_MAXP predicates (k_filter_scan,
+// a single-pass scan with decoupled look-back):
+//   * a CTA takes the next 4,096-row tile from a ticket counter, so every
+//     tile before it is already running or done;
+//   * its threads load the tile's labels and timestamps as float4 (16 rows
+//     each, coalesced) and evaluate every predicate on them;
+//   * per predicate the tile's passing count is published at once (flag
+//     AGGREGATE), the prefix of the tiles before it is read from their
+//     published words (one warp looks back 32 tiles at a time and stops at
+//     the nearest INCLUSIVE one), the tile's inclusive prefix is published,
+//     and every passing row writes its id at prefix + its rank in the tile.
+// A status word holds its flag and its value together, so one 64-bit
+// volatile load sees a consistent pair.  The waits on predecessors are
+// bounded by the global timer; a look-back that gives up marks its tile, so
+// the tiles after it give up too, and that predicate's count is UINT64_MAX.
 // Nothing is read back: the counts land in device memory, so a batch of
 // calls streams back to back.  Algorithmic traffic per launch: 8 B per row
-// plus 4 B per passing row; the kernels add N/4 bytes per predicate of
-// bit-array traffic, mostly in L2.
+// plus 4 B per passing row.
 #include <algorithm>
 #include <cstring>
 
@@ -26,13 +30,16 @@ namespace fknn {
 
 namespace {
 
-constexpr int FP_THREADS = 256;
-constexpr int FP_ITEMS = 8;
-constexpr int FP_CHUNK = FP_THREADS * FP_ITEMS;  // rows per chunk
-constexpr int FP_WORDS = FP_CHUNK / 32;          // bit words per chunk
-constexpr int FP_NW = FP_THREADS / 32;
-constexpr uint32_t FP_MAXP = 16;                 // predicates per launch
-constexpr int FP_CTAS_PER_SM = 8;                // resident at <= 32 registers: one wave
+constexpr int FS_THREADS = 256;
+constexpr int FS_NW = FS_THREADS / 32;
+constexpr int FS_IT = 4;                          // float4 loads per column per thread
+constexpr int FS_TILE = FS_THREADS * 4 * FS_IT;   // 4,096 rows per tile
+constexpr int FS_SEG = FS_IT * FS_NW;             // 128-row warp segments per tile (= 32)
+constexpr uint32_t FP_MAXP = 16;                  // predicates per launch
+constexpr uint64_t ST_AGG = 1ull << 62, ST_INC = 2ull << 62, ST_FLAGS = 3ull << 62;
+constexpr uint64_t ST_BAD = 1ull << 61;  // a tile whose look-back gave up: its successors give up too
+
+static_assert(FS_SEG == 32, "one warp scans the tile's segments");
 
 struct FilterPreds {
   float4 m[FP_MAXP];  // (type, v, l, r), checked on the host
@@ -49,123 +56,157 @@ __device__ __forceinline__ bool pred_pass(const float4 &m, int32_t lab, float t)
   }
 }
 
-__global__ void __launch_bounds__(FP_THREADS, FP_CTAS_PER_SM) k_filter_mark(const float *__restrict__ labels,
+__device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t *p) { return *(const volatile uint64_t *)p; }
+
+// status: np x ntiles words and the ticket after them, zeroed before the
+// launch.  Grid: ntiles CTAs.
+__global__ void __launch_bounds__(FS_THREADS) k_filter_scan(const float *__restrict__ labels,
                                                             const float *__restrict__ ts, uint64_t n,
-                                                            FilterPreds P, uint32_t np, uint64_t rows_per_cta,
-                                                            uint32_t *__restrict__ bits, uint64_t words_per_pred,
-                                                            uint32_t *__restrict__ cta_cnt) {
-  __shared__ uint32_t wcnt[FP_MAXP][FP_NW];
-  __shared__ float4 pm[FP_MAXP];  // the predicates, indexed at run time (kept out of local memory)
-  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  for (int i = tid; i < (int)(FP_MAXP * FP_NW); i += FP_THREADS) (&wcnt[0][0])[i] = 0;
-  if (tid < (int)FP_MAXP) pm[tid] = P.m[tid];
-  __syncthreads();
-  const uint64_t r0 = (uint64_t)blockIdx.x * rows_per_cta;
-  const uint64_t r1 = min(n, r0 + rows_per_cta);
-  for (uint64_t c0 = r0; c0 < r1; c0 += FP_CHUNK) {
-    int32_t lab[FP_ITEMS];
-    float t[FP_ITEMS];
-#pragma unroll
-    for (int i = 0; i < FP_ITEMS; ++i) {
-      const uint64_t r = c0 + (uint64_t)i * FP_THREADS + tid;
-      lab[i] = 0;
-      t[i] = 0.f;
-      if (r < r1) {
-        lab[i] = (int32_t)__ldcs(labels + r);
-        t[i] = __ldcs(ts + r);
-      }
-    }
-    for (uint32_t p = 0; p < np; ++p) {
-      const float4 m = pm[p];
-      uint32_t mine = 0, cnt = 0;
-#pragma unroll
-      for (int i = 0; i < FP_ITEMS; ++i) {
-        const uint64_t r = c0 + (uint64_t)i * FP_THREADS + tid;
-        const uint32_t b = __ballot_sync(0xffffffffu, r < r1 && pred_pass(m, lab[i], t[i]));
-        if (lane == i) mine = b;
-        cnt += __popc(b);
-      }
-      // word of rows c0 + lane*256 + w*32 .. +31
-      if (lane < FP_ITEMS && c0 + (uint64_t)lane * FP_THREADS + w * 32 < r1)
-        bits[p * words_per_pred + c0 / 32 + lane * FP_NW + w] = mine;
-      if (lane == 0) wcnt[p][w] += cnt;
-    }
-  }
-  __syncthreads();
-  if (tid < (int)np) {
-    uint32_t s = 0;
-#pragma unroll
-    for (int j = 0; j < FP_NW; ++j) s += wcnt[tid][j];
-    cta_cnt[(uint64_t)tid * gridDim.x + blockIdx.x] = s;
-  }
-}
-
-// Block-wide sum of one value per thread (all threads get it).
-__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t *red) {
-  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-  if (lane == 0) red[w] = v;
-  __syncthreads();
-  uint32_t s = 0;
-#pragma unroll
-  for (int j = 0; j < FP_NW; ++j) s += red[j];
-  __syncthreads();
-  return s;
-}
-
-__global__ void __launch_bounds__(FP_THREADS) k_filter_emit(uint64_t n, uint64_t rows_per_cta,
-                                                            const uint32_t *__restrict__ bits, uint64_t words_per_pred,
-                                                            const uint32_t *__restrict__ cta_cnt,
+                                                            FilterPreds P, uint32_t np, uint32_t ntiles,
+                                                            uint64_t *__restrict__ status, uint32_t *ticket,
                                                             uint32_t *__restrict__ out, uint64_t out_stride,
                                                             uint64_t *__restrict__ counts) {
-  __shared__ uint32_t red[FP_NW];
-  __shared__ uint32_t wsm[FP_WORDS], woff[FP_WORDS + 1];
+  __shared__ float4 pm[FP_MAXP];
+  __shared__ uint32_t seg[FS_SEG];
+  __shared__ uint32_t s_tile;
+  __shared__ uint64_t s_prefix;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  const uint32_t g = blockIdx.x, G = gridDim.x, p = blockIdx.y;
-  const uint32_t *cc = cta_cnt + (uint64_t)p * G;
-  uint32_t s = 0;
-  for (uint32_t j = tid; j < g; j += FP_THREADS) s += cc[j];
-  uint32_t base = block_sum(s, red);
-  const uint64_t r0 = (uint64_t)g * rows_per_cta;
-  const uint64_t r1 = min(n, r0 + rows_per_cta);
-  const uint32_t *bp = bits + (uint64_t)p * words_per_pred;
-  uint32_t *op = out + (uint64_t)p * out_stride;
-  const uint32_t lt = (1u << lane) - 1u;
-  for (uint64_t c0 = r0; c0 < r1; c0 += FP_CHUNK) {
-    // exclusive scan of the chunk's FP_WORDS word popcounts
-    if (tid < FP_WORDS) {
-      const uint32_t word = (c0 + (uint64_t)tid * 32 < r1) ? __ldcs(bp + c0 / 32 + tid) : 0u;
-      const uint32_t pc = __popc(word);
-      uint32_t inc = pc;
+  if (tid < (int)FP_MAXP) pm[tid] = P.m[tid];
+  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  __syncthreads();
+  const uint32_t t = s_tile;
+  const uint64_t base = (uint64_t)t * FS_TILE;
+  // this thread's rows: base + it*1024 + 4*tid + c, c = 0..3
+  int32_t lab[FS_IT][4];
+  float tv[FS_IT][4];
+  uint32_t valid = 0;  // bit it*4+c: the row is inside the base
+#pragma unroll
+  for (int it = 0; it < FS_IT; ++it) {
+    const uint64_t r = base + (uint64_t)it * (FS_THREADS * 4) + 4 * tid;
+    if (r + 4 <= n) {
+      const float4 a = __ldcs(reinterpret_cast<const float4 *>(labels + r));
+      const float4 b = __ldcs(reinterpret_cast<const float4 *>(ts + r));
+      lab[it][0] = (int32_t)a.x;
+      lab[it][1] = (int32_t)a.y;
+      lab[it][2] = (int32_t)a.z;
+      lab[it][3] = (int32_t)a.w;
+      tv[it][0] = b.x;
+      tv[it][1] = b.y;
+      tv[it][2] = b.z;
+      tv[it][3] = b.w;
+      valid |= 0xfu << (it * 4);
+    } else {
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        lab[it][c] = 0;
+        tv[it][c] = 0.f;
+        if (r + c < n) {
+          lab[it][c] = (int32_t)labels[r + c];
+          tv[it][c] = ts[r + c];
+          valid |= 1u << (it * 4 + c);
+        }
+      }
+    }
+  }
+  for (uint32_t p = 0; p < np; ++p) {
+    const float4 m = pm[p];
+    uint32_t mask = 0;
+#pragma unroll
+    for (int it = 0; it < FS_IT; ++it)
+#pragma unroll
+      for (int c = 0; c < 4; ++c) mask |= (pred_pass(m, lab[it][c], tv[it][c]) ? 1u : 0u) << (it * 4 + c);
+    mask &= valid;
+    // rank of this lane's rows inside its warp's 128-row segment of each it
+    uint32_t excl[FS_IT];
+#pragma unroll
+    for (int it = 0; it < FS_IT; ++it) {
+      const uint32_t cnt = __popc((mask >> (it * 4)) & 0xfu);
+      uint32_t inc = cnt;
 #pragma unroll
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
         if (lane >= o) inc += v;
       }
-      wsm[tid] = word;
-      woff[tid] = inc - pc;
-      if (lane == 31) red[w] = inc;
+      excl[it] = inc - cnt;
+      if (lane == 31) seg[it * FS_NW + w] = inc;
     }
     __syncthreads();
-    if (tid < FP_WORDS) {
-      uint32_t add = 0;
-      for (int j = 0; j < w; ++j) add += red[j];
-      woff[tid] += add;
-      if (tid == FP_WORDS - 1) woff[FP_WORDS] = woff[tid] + __popc(wsm[tid]);
-    }
-    __syncthreads();
+    if (w == 0) {
+      // the 32 segments in row order (it-major, then warp): exclusive offsets
+      const uint32_t v = seg[lane];
+      uint32_t inc = v;
 #pragma unroll
-    for (int i = 0; i < FP_ITEMS; ++i) {
-      const int wi = i * FP_NW + w;
-      const uint32_t word = wsm[wi];
-      if ((word >> lane) & 1u)
-        op[base + woff[wi] + __popc(word & lt)] = (uint32_t)(c0 + (uint64_t)i * FP_THREADS + tid);
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += x;
+      }
+      seg[lane] = inc - v;
+      const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
+      uint64_t *st = status + (uint64_t)p * ntiles;
+      uint64_t prefix = 0;
+      bool failed = false;
+      if (t > 0) {
+        if (lane == 0) {
+          __threadfence();
+          *(volatile uint64_t *)(st + t) = ST_AGG | total;
+        }
+        // look back 32 tiles at a time, down to the nearest tile that has
+        // published its inclusive prefix (before tile 0 the prefix is 0)
+        int64_t j = (int64_t)t - 1;
+        const uint64_t t0 = global_ns();
+        while (j >= 0) {
+          const int64_t jj = j - lane;
+          uint64_t sv = jj >= 0 ? ld_volatile_u64(st + jj) : ST_INC;
+          // every predecessor publishes its aggregate without waiting on
+          // anything, so these waits end; they are bounded all the same
+          // (every vote below is taken by all 32 lanes: the loop exits together)
+          while (true) {
+            const bool pending = (sv & ST_FLAGS) == 0;
+            if (!__any_sync(0xffffffffu, pending)) break;
+            if (__any_sync(0xffffffffu, global_ns() - t0 > WAIT_NS)) {
+              failed = true;
+              break;
+            }
+            if (pending) sv = ld_volatile_u64(st + jj);
+          }
+          if (failed) break;
+          const uint32_t inc_lanes = __ballot_sync(0xffffffffu, (sv & ST_FLAGS) == ST_INC);
+          const int stop = inc_lanes ? __ffs(inc_lanes) - 1 : 31;
+          if (__any_sync(0xffffffffu, lane <= stop && (sv & ST_BAD))) {
+            failed = true;
+            break;
+          }
+          uint64_t val = (lane <= stop && jj >= 0) ? (sv & 0xffffffffull) : 0ull;
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+          prefix += val;
+          if (inc_lanes) break;
+          j -= 32;
+        }
+      }
+      if (lane == 0) {
+        __threadfence();
+        *(volatile uint64_t *)(st + t) = failed ? (ST_INC | ST_BAD) : (ST_INC | ((prefix + total) & 0xffffffffull));
+        s_prefix = failed ? ~0ull : prefix;
+        if (t == ntiles - 1) counts[p] = failed ? ~0ull : prefix + total;
+      }
     }
-    base += woff[FP_WORDS];
     __syncthreads();
+    const uint64_t prefix = s_prefix;
+    if (prefix != ~0ull) {
+      uint32_t *op = out + (uint64_t)p * out_stride;
+#pragma unroll
+      for (int it = 0; it < FS_IT; ++it) {
+        const uint32_t mk = (mask >> (it * 4)) & 0xfu;
+        uint32_t pos = (uint32_t)prefix + seg[it * FS_NW + w] + excl[it];
+        const uint64_t r = base + (uint64_t)it * (FS_THREADS * 4) + 4 * tid;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if ((mk >> c) & 1u) op[pos++] = (uint32_t)(r + c);
+      }
+    }
+    __syncthreads();  // seg and s_prefix are rewritten for the next predicate
   }
-  if (g == G - 1 && tid == 0) counts[p] = base;
 }
 
 }  // namespace
@@ -192,17 +233,12 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
                       cudaStream_t st) {
   const uint64_t n = idx->n;
   if (np == 0) return FKNN_OK;
-  // equal row ranges, a multiple of 256 rows each, one resident wave of CTAs
-  const uint64_t g0 = std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)idx->num_sms * FP_CTAS_PER_SM,
-                                                                (n + FP_THREADS - 1) / FP_THREADS));
-  const uint64_t rows_per_cta = ((n + g0 - 1) / g0 + FP_THREADS - 1) / FP_THREADS * FP_THREADS;
-  const uint32_t G = (uint32_t)((n + rows_per_cta - 1) / rows_per_cta);
-  const uint64_t wpp = (G * rows_per_cta + 31) / 32;
+  const uint32_t ntiles = (uint32_t)((n + FS_TILE - 1) / FS_TILE);
   const uint32_t pmax = std::min<uint32_t>(np, FP_MAXP);
-  uint32_t *bits, *cnt;
+  // per launch: status words (predicates x tiles) and the ticket, cleared first
+  uint64_t *status;
   int rc;
-  if ((rc = ws_get(idx, 16, (size_t)pmax * wpp * 4 + 256, (void **)&bits))) return rc;
-  if ((rc = ws_get(idx, 17, (size_t)pmax * G * 4 + 256, (void **)&cnt))) return rc;
+  if ((rc = ws_get(idx, 16, ((size_t)pmax * ntiles + 1) * sizeof(uint64_t), (void **)&status))) return rc;
   for (uint32_t p0 = 0; p0 < np; p0 += FP_MAXP) {
     const uint32_t m = std::min<uint32_t>(FP_MAXP, np - p0);
     FilterPreds P;
@@ -211,10 +247,11 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
       const float *q = metas + (size_t)(p0 + p) * 4;
       P.m[p] = make_float4(q[0], q[1], q[2], q[3]);
     }
-    k_filter_mark<<<G, FP_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, P, m, rows_per_cta, bits, wpp, cnt);
-    k_filter_emit<<<dim3(G, m), FP_THREADS, 0, st>>>(n, rows_per_cta, bits, wpp, cnt, d_out + (uint64_t)p0 * n, n,
-                                                     d_counts + p0);
-    g_launches += 2;
+    uint32_t *ticket = reinterpret_cast<uint32_t *>(status + (size_t)m * ntiles);
+    FKNN_CUDA(cudaMemsetAsync(status, 0, ((size_t)m * ntiles + 1) * sizeof(uint64_t), st));
+    k_filter_scan<<<ntiles, FS_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, P, m, ntiles, status, ticket,
+                                                 d_out + (uint64_t)p0 * n, n, d_counts + p0);
+    g_launches += 1;
   }
   FKNN_CUDA(cudaGetLastError());
   return FKNN_OK;
@@ -229,6 +266,10 @@ int filter_rows(fknn_index *idx, const float *m4, uint32_t *d_out, uint64_t *cou
   uint64_t tot = 0;
   FKNN_CUDA(cudaMemcpyAsync(&tot, d_cnt, 8, cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
+  if (tot == ~0ull) {
+    set_error("fknn_filter_rows: a bounded device wait gave up");
+    return FKNN_ETIMEOUT;
+  }
   *count = tot;
   return FKNN_OK;
 }
