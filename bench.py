@@ -931,7 +931,8 @@ def main():
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "bf16" if use_bf16 else "f32", "data": "synthetic",
-            "config": {"workload": w.name, "mode": "bf16_rerank" if use_bf16 else "exact_fp32",
+            "config": {"workload": w.name if (n, nq) == (w.n, w.nq) else f"{w.name} resized to n={n}, nq={nq}",
+                       "mode": "bf16_rerank" if use_bf16 else "exact_fp32",
                        "kprime": args.kprime if use_bf16 else None, "n": n, "nq_per_gpu": nq, "k": 100, "d": 100,
                        "tuning": idx.get_tuning(head_mode),
                        "parallelism": f"replicas{world}" if world > 1 else "single",
