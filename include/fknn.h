@@ -73,9 +73,20 @@ typedef struct fknn_tuning {
                                 merge; exact: the k-th of the sample, a valid upper bound */
 } fknn_tuning;
 
+/* fknn_search_opts.flags */
+#define FKNN_SEARCH_GRAPH 1u /* reduced-precision modes: plan on the device and replay a captured CUDA graph */
+
 typedef struct fknn_search_opts {
   int mode;             /* FKNN_MODE_* */
   uint32_t kprime;      /* candidate width for the reduced-precision modes (0 = default 400) */
+  uint32_t flags;       /* FKNN_SEARCH_* bits, 0 = host-planned search.  FKNN_SEARCH_GRAPH:
+                         * the query grouping, tile and work-item plan are built by
+                         * kernels, every launch has a size fixed by (nq, index), and
+                         * the whole search is captured once into a CUDA graph that
+                         * later calls with the same nq, k, kprime, tuning and buffer
+                         * addresses replay (one graph launch + one flag read-back).
+                         * Results equal the host-planned search's up to the order of
+                         * equal-distance candidates.  Exact mode ignores the flag. */
 } fknn_search_opts;
 
 /* Per-call statistics (optional out-parameter of fknn_search_ex). */

@@ -18,6 +18,7 @@
 #include <cfloat>
 #include <chrono>
 #include <cstring>
+#include <vector>
 
 #include <cuda_bf16.h>
 #include <cuda_fp8.h>
@@ -125,25 +126,62 @@ __global__ void k_build_bf16_blocks(const float *__restrict__ vecs, const float 
   }
 }
 
-__global__ void k_tile_stage_bf16(const float *__restrict__ q, const int32_t *__restrict__ lane_q,
-                                  const QueryDesc *__restrict__ desc, __nv_bfloat16 *__restrict__ out,
-                                  float2 *__restrict__ lane_qs) {
-  constexpr int BK = FmtBF16::K;
-  const uint32_t t = blockIdx.x;
-  __nv_bfloat16 *o = out + (uint64_t)t * (BF_TILE / 2);
-  for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
-    const int32_t qi = lane_q[t * BQ + l];
-    lane_qs[t * BQ + l] = make_float2(qi >= 0 ? desc[qi].qn : 0.f, 1.f);
-  }
-  for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * BK; i += blockDim.x) {
-    const uint32_t l = i / BK, k = i % BK;
-    const int32_t qi = lane_q[t * BQ + l];
-    float v = 0.f;
+// Where a tile's lanes come from: the host plan's per-tile arrays, or a
+// device plan's sorted queries (tile t = positions tile_first[t] ..
+// + tiles[t].nq of order_q, slabs from the query descriptors).
+struct LaneSrc {
+  const int32_t *lane_q = nullptr;
+  const uint32_t *lane_s = nullptr, *lane_e = nullptr;
+  const uint32_t *tile_first = nullptr, *order_q = nullptr;
+  const QueryDesc *desc = nullptr;
+  const uint32_t *ntile = nullptr;  // device plan: the tile count
+};
+
+__device__ __forceinline__ int32_t lane_query(const LaneSrc &ls, const Tile &tl, uint32_t t, int L, uint32_t &s,
+                                              uint32_t &e) {
+  if (ls.lane_q) {
+    const int32_t qi = ls.lane_q[t * BQ + L];
     if (qi >= 0) {
-      if (k < (uint32_t)DIM) v = q[(uint64_t)qi * DIM + k];
-      else if (k == DIM || k == DIM + 1) v = 1.f;
+      s = ls.lane_s[t * BQ + L];
+      e = ls.lane_e[t * BQ + L];
     }
-    o[cm_index(l, k)] = __float2bfloat16_rn(v);
+    return qi;
+  }
+  if ((uint32_t)L >= tl.nq) return -1;
+  const int32_t qi = (int32_t)ls.order_q[ls.tile_first[t] + L];
+  s = ls.desc[qi].s;
+  e = ls.desc[qi].e;
+  return qi;
+}
+
+// One block per tile (grid-strided over a device plan's tile count).
+__global__ void k_tile_stage_bf16(const float *__restrict__ q, LaneSrc ls, const Tile *__restrict__ tiles,
+                                  uint32_t ntile_h, const QueryDesc *__restrict__ desc,
+                                  __nv_bfloat16 *__restrict__ out, float2 *__restrict__ lane_qs) {
+  constexpr int BK = FmtBF16::K;
+  const uint32_t ntile = ls.ntile ? *ls.ntile : ntile_h;
+  __shared__ int32_t lq[BQ];
+  for (uint32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    __nv_bfloat16 *o = out + (uint64_t)t * (BF_TILE / 2);
+    for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
+      uint32_t s_, e_;
+      const int32_t qi = lane_query(ls, tl, t, (int)l, s_, e_);
+      lq[l] = qi;
+      lane_qs[t * BQ + l] = make_float2(qi >= 0 ? desc[qi].qn : 0.f, 1.f);
+    }
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * BK; i += blockDim.x) {
+      const uint32_t l = i / BK, k = i % BK;
+      const int32_t qi = lq[l];
+      float v = 0.f;
+      if (qi >= 0) {
+        if (k < (uint32_t)DIM) v = q[(uint64_t)qi * DIM + k];
+        else if (k == DIM || k == DIM + 1) v = 1.f;
+      }
+      o[cm_index(l, k)] = __float2bfloat16_rn(v);
+    }
+    __syncthreads();
   }
 }
 
@@ -226,40 +264,47 @@ __global__ void k_build_fp8_blocks(const float *__restrict__ vecs, const uint32_
   }
 }
 
-__global__ void k_tile_stage_fp8(const float *__restrict__ q, const int32_t *__restrict__ lane_q,
-                                 const float *__restrict__ center, const float *__restrict__ scale,
+__global__ void k_tile_stage_fp8(const float *__restrict__ q, LaneSrc ls, const Tile *__restrict__ tiles,
+                                 uint32_t ntile_h, const float *__restrict__ center, const float *__restrict__ scale,
                                  unsigned char *__restrict__ out, float2 *__restrict__ lane_qs) {
-  const uint32_t t = blockIdx.x;
-  unsigned char *o = out + (uint64_t)t * F8_TILE;
+  const uint32_t ntile = ls.ntile ? *ls.ntile : ntile_h;
   __shared__ float lam[BQ];
-  for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
-    const int32_t qi = lane_q[t * BQ + l];
-    float qn = 0.f, mw = 0.f;
-    if (qi >= 0) {
-      const float *x = q + (uint64_t)qi * DIM;
-      for (int k = 0; k < DIM; ++k) {
-        const float u = x[k] - center[k];
-        qn = fmaf(u, u, qn);
-        mw = fmaxf(mw, fabsf(u * scale[k]));
+  __shared__ int32_t lq[BQ];
+  for (uint32_t t = blockIdx.x; t < ntile; t += gridDim.x) {
+    const Tile tl = tiles[t];
+    unsigned char *o = out + (uint64_t)t * F8_TILE;
+    for (uint32_t l = threadIdx.x; l < (uint32_t)BQ; l += blockDim.x) {
+      uint32_t s_, e_;
+      const int32_t qi = lane_query(ls, tl, t, (int)l, s_, e_);
+      lq[l] = qi;
+      float qn = 0.f, mw = 0.f;
+      if (qi >= 0) {
+        const float *x = q + (uint64_t)qi * DIM;
+        for (int k = 0; k < DIM; ++k) {
+          const float u = x[k] - center[k];
+          qn = fmaf(u, u, qn);
+          mw = fmaxf(mw, fabsf(u * scale[k]));
+        }
       }
+      // largest power of two with lambda * max|w| <= 448, within e4m3's exact powers
+      int e = 8;
+      if (mw > 0.f) e = min(8, max(-9, (int)floorf(log2f(448.f / mw))));
+      const float lambda = ldexpf(1.f, e);
+      lam[l] = lambda;
+      lane_qs[t * BQ + l] = make_float2(qn, 1.f / lambda);
     }
-    // largest power of two with lambda * max|w| <= 448, within e4m3's exact powers
-    int e = 8;
-    if (mw > 0.f) e = min(8, max(-9, (int)floorf(log2f(448.f / mw))));
-    const float lambda = ldexpf(1.f, e);
-    lam[l] = lambda;
-    lane_qs[t * BQ + l] = make_float2(qn, 1.f / lambda);
-  }
-  __syncthreads();
-  for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * FmtFP8::K; i += blockDim.x) {
-    const uint32_t l = i / FmtFP8::K, k = i % FmtFP8::K;
-    const int32_t qi = lane_q[t * BQ + l];
-    float v = 0.f;
-    if (qi >= 0) {
-      if (k < (uint32_t)DIM) v = lam[l] * (q[(uint64_t)qi * DIM + k] - center[k]) * scale[k];
-      else if (k <= DIM + 2) v = lam[l];
+    __syncthreads();
+    for (uint32_t i = threadIdx.x; i < (uint32_t)BQ * FmtFP8::K; i += blockDim.x) {
+      const uint32_t l = i / FmtFP8::K, k = i % FmtFP8::K;
+      const int32_t qi = lq[l];
+      float v = 0.f;
+      if (qi >= 0) {
+        if (k < (uint32_t)DIM) v = lam[l] * (q[(uint64_t)qi * DIM + k] - center[k]) * scale[k];
+        else if (k <= DIM + 2) v = lam[l];
+      }
+      o[cm_byte(l, k)] = __nv_fp8_e4m3(v).__x;
     }
-    o[cm_byte(l, k)] = __nv_fp8_e4m3(v).__x;
+    __syncthreads();
   }
 }
 
@@ -438,26 +483,24 @@ __device__ __noinline__ void bcompact(Candidate *list, BScreenSmem<F> &sm, int L
   __syncwarp();
 }
 
+// One CTA per resident slot; it works through the items blockIdx.x,
+// blockIdx.x + gridDim.x, ... (a host plan launches one CTA per item, a
+// device plan a fixed grid over the device item count).  The barrier
+// phases run on across items: g counts the sub-tiles this CTA has issued.
 template <class F, int NPL>
 __global__ void __launch_bounds__(B_THREADS, 2)
     k_screen_tc(const WorkItem *__restrict__ items, const Tile *__restrict__ tiles,
-                  const unsigned char *__restrict__ atiles, const int32_t *__restrict__ lane_q,
-                  const uint32_t *__restrict__ lane_s, const uint32_t *__restrict__ lane_e,
-                  const float2 *__restrict__ lane_qs, const unsigned char *__restrict__ blocks_t,
-                  const unsigned char *__restrict__ blocks_c, uint32_t *__restrict__ T_global,
-                  uint32_t *__restrict__ ovf, Candidate *__restrict__ out, uint32_t *__restrict__ out_cnt,
-                  uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride, uint32_t withhold,
-                  int *err) {
+                const unsigned char *__restrict__ atiles, LaneSrc ls, const float2 *__restrict__ lane_qs,
+                const unsigned char *__restrict__ blocks_t, const unsigned char *__restrict__ blocks_c,
+                uint32_t *__restrict__ T_global, uint32_t *__restrict__ ovf, Candidate *__restrict__ out,
+                uint32_t *__restrict__ out_cnt, uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride,
+                uint32_t withhold, uint32_t nitems_h, const uint32_t *__restrict__ nitems_d, int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   BScreenSmem<F> &sm = *reinterpret_cast<BScreenSmem<F> *>(smem_raw);
   constexpr uint32_t TB = Tiles<F>::BYTES;
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-  const uint32_t item_id = blockIdx.x;
-  const WorkItem it = items[item_id];
-  const Tile tl = tiles[it.tile];
-  const unsigned char *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
-  // every stride-th row block of the item (stride 1: all of them)
-  const uint32_t nsub = (it.blk1 - it.blk0 + stride - 1) / stride;
+  const uint32_t nitems = nitems_d ? *nitems_d : nitems_h;
+  if (blockIdx.x >= nitems) return;  // (uniform: before any barrier or TMEM use)
 
   if (tid == 0) {
     for (int s = 0; s < BS; ++s) {
@@ -481,156 +524,185 @@ __global__ void __launch_bounds__(B_THREADS, 2)
   tc_fence_after();
   const uint32_t tmem = sm.tmem_base;
 
-  if (warp == 0) {
-    // ------------------------------------------------ producer
-    if (lane == 0) {
-      mbar_arrive_expect_tx(&sm.abar, TB);
-      bulk_g2s(sm.a, atiles + (uint64_t)it.tile * TB, TB, &sm.abar);
-      uint32_t issued = 0;
-      // test hook (fknn_index_test_withhold_copy): the first work item issues
-      // no row-block copy, so its MMA issuer's and epilogue's waits run out
-      const uint32_t nsub_issue = (withhold && item_id == 0) ? 0u : nsub;
-      for (uint32_t sub = 0; sub < nsub_issue; ++sub) {
-        const int st = sub % BS;
-        if (sub >= BS && !mbar_wait_bounded(&sm.empty[st], ((sub / BS) - 1) & 1, err)) break;
-        mbar_arrive_expect_tx(&sm.full[st], TB);
-        bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub * stride) * TB, TB, &sm.full[st]);
-        ++issued;
-      }
-      mbar_wait_bounded(&sm.abar, 0, err);
-      for (uint32_t i = issued > BS ? issued - BS : 0; i < issued; ++i)
-        mbar_wait_bounded(&sm.full[i % BS], (i / BS) & 1, err);
-    }
-  } else if (warp == 1) {
-    // ------------------------------------------------ MMA issuer
-    if (lane == 0) {
-      uint32_t done = 0;
-      if (mbar_wait_bounded(&sm.abar, 0, err)) {
-        const uint32_t a0 = smem_u32(sm.a);
-        for (uint32_t sub = 0; sub < nsub; ++sub) {
-          const int st = sub % BS, ab = sub & 1;
-          if (!mbar_wait_bounded(&sm.full[st], (sub / BS) & 1, err)) break;
-          if (sub >= 2 && !mbar_wait_bounded(&sm.accempty[ab], ((sub >> 1) - 1) & 1, err)) break;
-          tc_fence_after();
-          const uint32_t b0 = smem_u32(sm.b[st]);
-#pragma unroll
-          for (int kk = 0; kk < F::MMAS; ++kk) {
-            const uint64_t da = umma_desc(a0 + kk * 2 * (BQ / 8) * 128, (BQ / 8) * 128, 128);
-            const uint64_t db = umma_desc(b0 + kk * 2 * (BR / 8) * 128, (BR / 8) * 128, 128);
-            umma<F>(tmem + ab * BR, da, db, kk > 0);
+  uint32_t g = 0;  // sub-tiles of this CTA's earlier items
+  uint32_t iter = 0;
+  // a bounded wait gave up: the CTA's later items only mark their queries
+  // (combined over the block at each item's closing barrier, so uniform)
+  bool aborted = false;
+  for (uint32_t item_id = blockIdx.x; item_id < nitems; item_id += gridDim.x, ++iter) {
+    const WorkItem it = items[item_id];
+    const Tile tl = tiles[it.tile];
+    const unsigned char *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
+    // every stride-th row block of the item (stride 1: all of them)
+    const uint32_t nsub = (it.blk1 - it.blk0 + stride - 1) / stride;
+    bool gave_up = false;  // this thread saw a wait give up in this item
+
+    if (warp == 0) {
+      // ------------------------------------------------ producer
+      if (lane == 0 && !aborted) {
+        bool ok = true;
+        mbar_arrive_expect_tx(&sm.abar, TB);
+        bulk_g2s(sm.a, atiles + (uint64_t)it.tile * TB, TB, &sm.abar);
+        uint32_t issued = 0;
+        // test hook (fknn_index_test_withhold_copy): the first work item issues
+        // no row-block copy, so its MMA issuer's and epilogue's waits run out
+        const uint32_t nsub_issue = (withhold && item_id == 0) ? 0u : nsub;
+        for (uint32_t sub = 0; sub < nsub_issue; ++sub) {
+          const uint32_t gs = g + sub;
+          const int st = gs % BS;
+          if (gs >= BS && !mbar_wait_bounded(&sm.empty[st], ((gs / BS) - 1) & 1, err)) {
+            ok = false;
+            break;
           }
-          umma_commit(&sm.empty[st]);     // the row block may be overwritten once these MMAs finish
-          umma_commit(&sm.accfull[ab]);   // the accumulator is ready for the epilogue
-          ++done;
+          mbar_arrive_expect_tx(&sm.full[st], TB);
+          bulk_g2s(sm.b[st], blocks + (uint64_t)(it.blk0 + sub * stride) * TB, TB, &sm.full[st]);
+          ++issued;
+        }
+        // every issued copy has landed before the item ends
+        ok = mbar_wait_bounded(&sm.abar, iter & 1, err) && ok;
+        for (uint32_t i = issued > BS ? issued - BS : 0; i < issued; ++i)
+          ok = mbar_wait_bounded(&sm.full[(g + i) % BS], ((g + i) / BS) & 1, err) && ok;
+        if (!ok || issued != nsub) gave_up = true;
+      }
+    } else if (warp == 1) {
+      // ------------------------------------------------ MMA issuer
+      if (lane == 0 && !aborted) {
+        uint32_t done = 0;
+        if (mbar_wait_bounded(&sm.abar, iter & 1, err)) {
+          const uint32_t a0 = smem_u32(sm.a);
+          for (uint32_t sub = 0; sub < nsub; ++sub) {
+            const uint32_t gs = g + sub;
+            const int st = gs % BS, ab = gs & 1;
+            if (!mbar_wait_bounded(&sm.full[st], (gs / BS) & 1, err)) break;
+            if (gs >= 2 && !mbar_wait_bounded(&sm.accempty[ab], ((gs >> 1) - 1) & 1, err)) break;
+            tc_fence_after();
+            const uint32_t b0 = smem_u32(sm.b[st]);
+#pragma unroll
+            for (int kk = 0; kk < F::MMAS; ++kk) {
+              const uint64_t da = umma_desc(a0 + kk * 2 * (BQ / 8) * 128, (BQ / 8) * 128, 128);
+              const uint64_t db = umma_desc(b0 + kk * 2 * (BR / 8) * 128, (BR / 8) * 128, 128);
+              umma<F>(tmem + ab * BR, da, db, kk > 0);
+            }
+            umma_commit(&sm.empty[st]);     // the row block may be overwritten once these MMAs finish
+            umma_commit(&sm.accfull[ab]);   // the accumulator is ready for the epilogue
+            ++done;
+          }
+        }
+        // no MMA of this item is in flight when the next item (or the dealloc) comes
+        if (done) {
+          const uint32_t gl = g + done - 1;
+          mbar_wait_bounded(&sm.accfull[gl & 1], (gl >> 1) & 1, err);
+        }
+        if (done != nsub) gave_up = true;
+      }
+    } else {
+      // ------------------------------------------------ epilogue: thread = query
+      const int wslot = warp - 2;
+      const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
+      const int L = wg * 32 + lane;
+      uint32_t s = 0, e = 0;
+      const int32_t qi = lane_query(ls, tl, it.tile, L, s, e);
+      // per query: |q|^2 (centred for FP8) and the accumulator's scale 1/lambda
+      const float2 qsc = lane_qs[it.tile * BQ + L];
+      const float qn = qsc.x, sc = qsc.y;
+      float T = -INFINITY;
+      if (qi >= 0) {
+        T = sortable_f32(ld_volatile_u32(T_global + qi));
+        if (ld_volatile_u32(ovf + qi)) T = -INFINITY;
+      }
+      sm.lq[L] = qi;
+      sm.cnt[L] = 0;
+      sm.thr[L] = T;
+      __syncwarp();
+      Candidate *list = out + ((uint64_t)item_id * BQ + L) * capb;
+      int cnt = 0;
+      bool ok = !aborted;
+      for (uint32_t sub = 0; sub < nsub && ok; ++sub) {
+        const uint32_t gs = g + sub;
+        const int ab = gs & 1;
+        // warp-uniform: the lanes' timers may disagree at the deadline
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&sm.accfull[ab], (gs >> 1) & 1, err))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const uint32_t p0 = (it.blk0 + sub * stride) * BR;
+        const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
+        const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
+        // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc);
+        // with no bound yet every column of the slab is one (cq = -FLT_MAX),
+        // and columns outside the slab are -inf, which no cq admits
+        const float cq = (T == INFINITY) ? -FLT_MAX : 0.5f * (qn - T) / sc;
+        // four 32-column chunks; the TMEM load of the next chunk is in flight
+        // while this one is screened
+        const uint32_t tb = tmem + ((uint32_t)(wg * 32) << 16) + ab * BR;
+        uint32_t ra[32], rb[32];
+        tmem_ld32_issue(tb, ra);
+        tmem_wait_ld(ra);
+        tmem_ld32_issue(tb + 32, rb);
+        cnt = screen_chunk(ra, 0, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+        __syncwarp();
+        tmem_wait_ld(rb);
+        tmem_ld32_issue(tb + 64, ra);
+        cnt = screen_chunk(rb, 32, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+        __syncwarp();
+        tmem_wait_ld(ra);
+        tmem_ld32_issue(tb + 96, rb);
+        cnt = screen_chunk(ra, 64, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+        __syncwarp();
+        tmem_wait_ld(rb);
+        cnt = screen_chunk(rb, 96, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0) mbar_arrive1(&sm.accempty[ab]);
+        // lists that could overflow in the next sub-tile are bounded and
+        // trimmed; counts and bounds pass through shared memory only then
+        uint32_t msk = __ballot_sync(0xffffffffu, cnt > (int)capb - BR);
+        if (msk) {
+          sm.cnt[L] = cnt;
+          __syncwarp();
+          while (msk) {
+            const int b = __ffs(msk) - 1;
+            msk &= msk - 1;
+            const int Lb = wg * 32 + b;
+            bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+          }
+          cnt = sm.cnt[L];
+          T = sm.thr[L];
+        }
+        // other items of the same query tighten the shared bound meanwhile
+        if (refresh && sub % refresh == refresh - 1 && qi >= 0) {
+          const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+          if (Tg < T) {
+            T = Tg;
+            sm.thr[L] = T;
+          }
         }
       }
-      // no MMA may be in flight when TMEM is released
-      if (done) mbar_wait_bounded(&sm.accfull[(done - 1) & 1], ((done - 1) >> 1) & 1, err);
-    }
-  } else {
-    // ------------------------------------------------ epilogue: thread = query
-    const int wslot = warp - 2;
-    const int wg = warp & 3;  // TMEM lanes 32*wg .. 32*wg+31 are reachable from this warp
-    const int L = wg * 32 + lane;
-    const int32_t qi = lane_q[it.tile * BQ + L];
-    // per query: |q|^2 (centred for FP8) and the accumulator's scale 1/lambda
-    const float2 qsc = lane_qs[it.tile * BQ + L];
-    const float qn = qsc.x, sc = qsc.y;
-    uint32_t s = 0, e = 0;
-    float T = -INFINITY;
-    if (qi >= 0) {
-      s = lane_s[it.tile * BQ + L];
-      e = lane_e[it.tile * BQ + L];
-      T = sortable_f32(ld_volatile_u32(T_global + qi));
-      if (ld_volatile_u32(ovf + qi)) T = -INFINITY;
-    }
-    sm.lq[L] = qi;
-    sm.cnt[L] = 0;
-    sm.thr[L] = T;
-    __syncwarp();
-    Candidate *list = out + ((uint64_t)item_id * BQ + L) * capb;
-    int cnt = 0;
-    bool ok = true;
-    for (uint32_t sub = 0; sub < nsub; ++sub) {
-      const int ab = sub & 1;
-      if (!mbar_wait_bounded(&sm.accfull[ab], (sub >> 1) & 1, err)) {
-        ok = false;
-        break;
-      }
-      tc_fence_after();
-      const uint32_t p0 = (it.blk0 + sub * stride) * BR;
-      const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
-      const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
-      // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc);
-      // with no bound yet every column of the slab is one (cq = -FLT_MAX),
-      // and columns outside the slab are -inf, which no cq admits
-      const float cq = (T == INFINITY) ? -FLT_MAX : 0.5f * (qn - T) / sc;
-      // four 32-column chunks; the TMEM load of the next chunk is in flight
-      // while this one is screened
-      const uint32_t tb = tmem + ((uint32_t)(wg * 32) << 16) + ab * BR;
-      uint32_t ra[32], rb[32];
-      tmem_ld32_issue(tb, ra);
-      tmem_wait_ld(ra);
-      tmem_ld32_issue(tb + 32, rb);
-      cnt = screen_chunk(ra, 0, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
-      __syncwarp();
-      tmem_wait_ld(rb);
-      tmem_ld32_issue(tb + 64, ra);
-      cnt = screen_chunk(rb, 32, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
-      __syncwarp();
-      tmem_wait_ld(ra);
-      tmem_ld32_issue(tb + 96, rb);
-      cnt = screen_chunk(ra, 64, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
-      __syncwarp();
-      tmem_wait_ld(rb);
-      cnt = screen_chunk(rb, 96, r0, r1, cq, qn, sc, p0, &sm.stage[wslot][lane * STAGE_ROW], list, cnt);
-      tc_fence_before();
-      __syncwarp();
-      if (lane == 0) mbar_arrive1(&sm.accempty[ab]);
-      // lists that could overflow in the next sub-tile are bounded and
-      // trimmed; counts and bounds pass through shared memory only then
-      uint32_t msk = __ballot_sync(0xffffffffu, cnt > (int)capb - BR);
-      if (msk) {
+      if (!ok) {
+        // this item's queries are answered by the exact scan
+        if (qi >= 0) ovf[qi] = 1u;
+        out_cnt[(uint64_t)item_id * BQ + L] = 0;
+        gave_up = true;
+      } else {
         sm.cnt[L] = cnt;
         __syncwarp();
-        while (msk) {
-          const int b = __ffs(msk) - 1;
-          msk &= msk - 1;
+        for (int b = 0; b < 32; ++b) {
           const int Lb = wg * 32 + b;
-          bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
+          if (sm.cnt[Lb] > 0 && sm.lq[Lb] >= 0)
+            bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global,
+                             ovf);
         }
-        cnt = sm.cnt[L];
-        T = sm.thr[L];
-      }
-      // other items of the same query tighten the shared bound meanwhile
-      if (refresh && sub % refresh == refresh - 1 && qi >= 0) {
-        const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
-        if (Tg < T) {
-          T = Tg;
-          sm.thr[L] = T;
-        }
+        out_cnt[(uint64_t)item_id * BQ + L] = (uint32_t)sm.cnt[L];
       }
     }
-    if (!ok) {
-      if (qi >= 0) ovf[qi] = 1u;
-      out_cnt[(uint64_t)item_id * BQ + L] = 0;
-    } else {
-      sm.cnt[L] = cnt;
-      __syncwarp();
-      for (int b = 0; b < 32; ++b) {
-        const int Lb = wg * 32 + b;
-        if (sm.cnt[Lb] > 0 && sm.lq[Lb] >= 0)
-          bcompact<F, NPL>(out + ((uint64_t)item_id * BQ + Lb) * capb, sm, Lb, wslot, kprime, capb, T_global, ovf);
-      }
-      out_cnt[(uint64_t)item_id * BQ + L] = (uint32_t)sm.cnt[L];
-    }
-  }
-  tc_fence_before();
-  __syncthreads();
-  if (warp == 1) {
+    g += nsub;
+    tc_fence_before();
+    // the item's shared state (A tile, lists' counts, bounds) is reused by the next
+    aborted = __syncthreads_or(aborted || gave_up) != 0;
     tc_fence_after();
-    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
   }
+  if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
 
 // ------------------------------------------------------------ re-rank --
@@ -665,6 +737,7 @@ struct MergeArgs {
   uint32_t *ids;
   float *dists;
   uint32_t *n_f64;
+  const uint32_t *nbig_d;  // device plan: the big-query count (NULL: the launch's nbig)
 };
 
 // One big query b (index into the plan's big-query arrays): gather its
@@ -801,7 +874,7 @@ __global__ void __launch_bounds__(RR_THREADS)
                    uint32_t *__restrict__ spill_count) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   RerankSmem<CAP> &sm = *reinterpret_cast<RerankSmem<CAP> *>(smem_raw);
-  const uint32_t nwork = work ? *work_count : nbig;
+  const uint32_t nwork = work ? *work_count : (A.nbig_d ? *A.nbig_d : nbig);
   for (uint32_t w = blockIdx.x; w < nwork; w += gridDim.x) {
     merge_one<CAP>(A, work ? work[w] : w, sm, spill, spill_count);
     __syncthreads();  // shared memory is reused by the next query
@@ -812,9 +885,11 @@ __global__ void __launch_bounds__(RR_THREADS)
 // the r-th smallest screening distance over every stride-th row block, an
 // estimate of the k'-th over all rows (r is chosen so that it lies above it
 // with high probability; the merge catches the rest).
-__global__ void k_seed_bounds(const uint32_t *__restrict__ big_q, uint32_t nbig, const QueryDesc *__restrict__ desc,
-                              const uint32_t *__restrict__ T_A, const uint32_t *__restrict__ ovf_A,
-                              uint32_t min_rows, uint32_t *__restrict__ T_global, uint32_t *__restrict__ seeded) {
+__global__ void k_seed_bounds(const uint32_t *__restrict__ big_q, uint32_t nbig_h, const uint32_t *__restrict__ nbig_d,
+                              const QueryDesc *__restrict__ desc, const uint32_t *__restrict__ T_A,
+                              const uint32_t *__restrict__ ovf_A, uint32_t min_rows, uint32_t *__restrict__ T_global,
+                              uint32_t *__restrict__ seeded) {
+  const uint32_t nbig = nbig_d ? *nbig_d : nbig_h;
   for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nbig; i += gridDim.x * blockDim.x) {
     const uint32_t qi = big_q[i];
     const uint32_t inf = f32_sortable(INFINITY);
@@ -959,12 +1034,16 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
     if ((rc = ws_get(idx, 10, (size_t)ntile * BQ * sizeof(float2), (void **)&d_lqs))) return rc;
     if ((rc = ws_get(idx, 6, (size_t)nitems * BQ * capb * sizeof(Candidate), (void **)&d_out))) return rc;
     if ((rc = ws_get(idx, 7, (size_t)nitems * BQ * 4, (void **)&d_ocnt))) return rc;
+    LaneSrc ls;
+    ls.lane_q = (const int32_t *)(d_blob + o_lq);
+    ls.lane_s = (const uint32_t *)(d_blob + o_ls);
+    ls.lane_e = (const uint32_t *)(d_blob + o_le);
     if constexpr (F::kFP8)
-      k_tile_stage_fp8<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), idx->fp8_scale,
+      k_tile_stage_fp8<<<ntile, 256, 0, st>>>(d_q, ls, (const Tile *)(d_blob + o_tiles), ntile, idx->fp8_scale,
                                               idx->fp8_scale + DIM, d_at, d_lqs);
     else
-      k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, (const int32_t *)(d_blob + o_lq), d_desc, (__nv_bfloat16 *)d_at,
-                                               d_lqs);
+      k_tile_stage_bf16<<<ntile, 256, 0, st>>>(d_q, ls, (const Tile *)(d_blob + o_tiles), ntile, d_desc,
+                                               (__nv_bfloat16 *)d_at, d_lqs);
     // per device context, so set on every call (cheap)
     // the compaction holds a whole list in registers: 32 x NPL >= capb
     auto screen = capb <= 512 ? k_screen_tc<F, 16> : capb <= 768 ? k_screen_tc<F, 24>
@@ -988,19 +1067,17 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
       if ((rc = launch_fill_u32(T_A, nq, f32_sortable(INFINITY), st))) return rc;
       FKNN_CUDA(cudaMemsetAsync(ovf_A, 0, (size_t)nq * 4, st));
       screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
-          (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at,
-          (const int32_t *)(d_blob + o_lq), (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le),
-          d_lqs, (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A,
-          d_out, d_ocnt, r, capb, 0, stride, 0u, idx->d_flag);
+          (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, ls, d_lqs,
+          (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A, d_out,
+          d_ocnt, r, capb, 0, stride, 0u, nitems, nullptr, idx->d_flag);
       k_seed_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>((nbig + 255) / 256, 1184)), 256, 0, st>>>(
-          (const uint32_t *)(d_blob + o_big), nbig, d_desc, T_A, ovf_A, 16 * stride * BR, T_global, seeded);
+          (const uint32_t *)(d_blob + o_big), nbig, nullptr, d_desc, T_A, ovf_A, 16 * stride * BR, T_global, seeded);
       g_launches += 3;
     }
     screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
-        (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, (const int32_t *)(d_blob + o_lq),
-        (const uint32_t *)(d_blob + o_ls), (const uint32_t *)(d_blob + o_le), d_lqs,
+        (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, ls, d_lqs,
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
-        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->test_withhold ? 1u : 0u, idx->d_flag);
+        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->test_withhold ? 1u : 0u, nitems, nullptr, idx->d_flag);
     idx->test_withhold = false;
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     MergeArgs A;
@@ -1026,6 +1103,7 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
     A.ids = d_ids;
     A.dists = d_dists;
     A.n_f64 = n_f64;
+    A.nbig_d = nullptr;
     // queries with more candidates than the common merge holds go to the large one
     uint32_t *spill = spill_count + 1;
     k_merge_rerank<RR_CAP_SMALL><<<nbig, RR_THREADS, sizeof(RerankSmem<RR_CAP_SMALL>), st>>>(
@@ -1068,9 +1146,230 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
   return FKNN_OK;
 }
 
+// The same search with the plan built on the device (device_plan.cu) and
+// every launch of fixed size, captured once into a CUDA graph and replayed
+// while nq, k, k', the tuning, the pointers and the scratch buffers stay
+// the same.  Screens run persistent over the device item count; merges and
+// scans read their counts from device memory.
+template <class F>
+static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k,
+                           uint32_t kprime, uint32_t *d_ids, float *d_dists, cudaStream_t st,
+                           fknn_search_stats *stats) {
+  constexpr uint32_t TB = Tiles<F>::BYTES;
+  int rc;
+  const fknn_tuning tune = idx->tuning[F::kFP8 ? FKNN_MODE_FP8_RERANK : FKNN_MODE_BF16_RERANK];
+  const uint32_t capb =
+      (uint32_t)std::min<size_t>(1280, align_up(kprime + std::max<uint32_t>(tune.list_slack, 2 * BR), 128));
+  PlanShape shape;
+  shape.tq = BQ;
+  shape.blk_rows = BR;
+  shape.small_slab = SMALL_SLAB;
+  shape.min_chunk_blocks = tune.min_chunk_blocks;
+  shape.target_items = idx->num_sms * tune.items_per_sm;
+  DevPlanSizes z = device_plan_sizes(idx, nq, shape);
+  const uint64_t per_item = (uint64_t)BQ * capb * sizeof(Candidate);
+  shape.max_items_per_tile = (uint32_t)std::max<uint64_t>(
+      1, std::min<uint64_t>(RR_CAP / capb, (8ull << 30) / (per_item * z.ntile_max)));
+  // all buffers exist before the capture (a capture may not allocate)
+  QueryDesc *d_desc;
+  void *d_plan;
+  unsigned char *d_at;
+  float2 *d_lqs;
+  Candidate *d_out;
+  uint32_t *d_ocnt, *d_state, *d_pilot = nullptr;
+  if ((rc = ws_get(idx, 2, (size_t)nq * sizeof(QueryDesc), (void **)&d_desc))) return rc;
+  if ((rc = ws_get(idx, 19, device_plan_bytes(nq, z), &d_plan))) return rc;
+  if ((rc = ws_get(idx, 4, (size_t)z.ntile_max * TB, (void **)&d_at))) return rc;
+  if ((rc = ws_get(idx, 10, (size_t)z.ntile_max * BQ * sizeof(float2), (void **)&d_lqs))) return rc;
+  if ((rc = ws_get(idx, 6, (size_t)z.nitems_max * per_item, (void **)&d_out))) return rc;
+  if ((rc = ws_get(idx, 7, (size_t)z.nitems_max * BQ * 4, (void **)&d_ocnt))) return rc;
+  if ((rc = ws_get(idx, 5, (size_t)nq * 16 + 64, (void **)&d_state))) return rc;
+  const uint32_t stride = tune.pilot_stride;
+  if (stride > 1 && (rc = ws_get(idx, 11, (size_t)nq * 12, (void **)&d_pilot))) return rc;
+  {  // the radix sort's histogram slot at its largest (the plan sorts nq keys)
+    void *h;
+    if ((rc = ws_get(idx, 15, ((size_t)(nq + 4095) / 4096) * 256 * sizeof(uint32_t) + 256, &h))) return rc;
+  }
+  DevPlan P;
+  device_plan_layout(P, d_plan, nq, z);
+  auto screen = capb <= 512 ? k_screen_tc<F, 16> : capb <= 768 ? k_screen_tc<F, 24>
+              : capb <= 1024 ? k_screen_tc<F, 32> : k_screen_tc<F, 40>;
+  FKNN_CUDA(cudaFuncSetAttribute(screen, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(BScreenSmem<F>)));
+  FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank<RR_CAP_SMALL>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(RerankSmem<RR_CAP_SMALL>)));
+  FKNN_CUDA(cudaFuncSetAttribute(k_merge_rerank<RR_CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sizeof(RerankSmem<RR_CAP>)));
+  GraphCache &G = idx->graph;
+  const bool withhold = idx->test_withhold;
+  idx->test_withhold = false;
+  const std::vector<uint64_t> key = {
+      (uint64_t)F::kFP8, nq, k, kprime, capb, tune.list_slack, tune.items_per_sm, tune.min_chunk_blocks,
+      tune.bound_refresh, tune.pilot_stride, (uint64_t)withhold, (uint64_t)(uintptr_t)d_q, (uint64_t)(uintptr_t)d_meta,
+      (uint64_t)(uintptr_t)d_ids, (uint64_t)(uintptr_t)d_dists, (uint64_t)(uintptr_t)d_desc,
+      (uint64_t)(uintptr_t)d_plan, (uint64_t)(uintptr_t)d_at, (uint64_t)(uintptr_t)d_lqs, (uint64_t)(uintptr_t)d_out,
+      (uint64_t)(uintptr_t)d_ocnt, (uint64_t)(uintptr_t)d_state, (uint64_t)(uintptr_t)d_pilot,
+      (uint64_t)(uintptr_t)idx->ws[15].p};
+  if (!G.exec || G.key != key) {
+    G.release();
+    for (auto &e : G.ev) FKNN_CUDA(cudaEventCreate(&e));
+    if (!G.cap) FKNN_CUDA(cudaStreamCreateWithFlags(&G.cap, cudaStreamNonBlocking));
+    const uint32_t l0 = g_launches;
+    const cudaStream_t user_st = st;
+    st = G.cap;  // captured nodes carry no stream: the replay goes to the caller's
+    FKNN_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+    // everything below is enqueued only; a failure ends the capture first
+    auto body = [&]() -> int {
+      int r;
+      if ((r = enqueue_query_prep(idx, d_q, d_meta, nq, d_desc, st))) return r;
+      if ((r = device_plan_build(idx, d_desc, d_meta, P, shape, st))) return r;
+      uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
+               *ovf_count = d_state + 3 * (size_t)nq, *n_f64 = ovf_count + 1, *spill_count = ovf_count + 2;
+      if ((r = launch_fill_u32(T_global, nq, f32_sortable(INFINITY), st))) return r;
+      FKNN_CUDA(cudaMemsetAsync(ovf, 0, (size_t)nq * 4, st));
+      FKNN_CUDA(cudaMemsetAsync(ovf_count, 0, 12, st));
+      const OrderData &OT = idx->ord[ORDER_TIME], &OC = idx->ord[ORDER_CAT];
+      LaneSrc ls;
+      ls.tile_first = P.tile_first;
+      ls.order_q = P.vals;
+      ls.desc = d_desc;
+      ls.ntile = P.cnt + DP_NTILE;
+      const unsigned tgrid = std::min<uint32_t>(z.ntile_max, (uint32_t)idx->num_sms * 4);
+      if constexpr (F::kFP8)
+        k_tile_stage_fp8<<<tgrid, 256, 0, st>>>(d_q, ls, P.tiles, 0, idx->fp8_scale, idx->fp8_scale + DIM, d_at,
+                                                d_lqs);
+      else
+        k_tile_stage_bf16<<<tgrid, 256, 0, st>>>(d_q, ls, P.tiles, 0, d_desc, (__nv_bfloat16 *)d_at, d_lqs);
+      g_launches += 1;
+      FKNN_CUDA(cudaEventRecord(G.ev[0], st));
+      void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
+      const unsigned sgrid = std::min<uint32_t>(z.nitems_max, (uint32_t)idx->num_sms * 2);
+      uint32_t *seeded = nullptr;
+      if (stride > 1) {
+        const uint32_t rr = std::min<uint32_t>(kprime, (3 * kprime + stride - 1) / stride + 8);
+        uint32_t *T_A = d_pilot, *ovf_A = d_pilot + 2 * (size_t)nq;
+        seeded = d_pilot + nq;
+        FKNN_CUDA(cudaMemsetAsync(seeded, 0, (size_t)nq * 4, st));
+        if ((r = launch_fill_u32(T_A, nq, f32_sortable(INFINITY), st))) return r;
+        FKNN_CUDA(cudaMemsetAsync(ovf_A, 0, (size_t)nq * 4, st));
+        screen<<<sgrid, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
+            P.items, P.tiles, d_at, ls, d_lqs, (const unsigned char *)blocks[ORDER_TIME],
+            (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A, d_out, d_ocnt, rr, capb, 0, stride, 0u, 0,
+            P.cnt + DP_NITEMS, idx->d_flag);
+        k_seed_bounds<<<1184, 256, 0, st>>>(P.big_q, 0, P.cnt + DP_NBIG, d_desc, T_A, ovf_A, 16 * stride * BR,
+                                            T_global, seeded);
+        g_launches += 2;
+      }
+      screen<<<sgrid, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
+          P.items, P.tiles, d_at, ls, d_lqs, (const unsigned char *)blocks[ORDER_TIME],
+          (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out, d_ocnt, kprime, capb, tune.bound_refresh, 1,
+          withhold ? 1u : 0u, 0, P.cnt + DP_NITEMS, idx->d_flag);
+      g_launches += 1;
+      FKNN_CUDA(cudaEventRecord(G.ev[1], st));
+      MergeArgs A;
+      A.big_q = P.big_q;
+      A.big_tile = P.big_tile;
+      A.big_lane = P.big_lane;
+      A.tiles = P.tiles;
+      A.item_slot = nullptr;  // a tile's items are consecutive
+      A.out = d_out;
+      A.out_cnt = d_ocnt;
+      A.desc = d_desc;
+      A.q = d_q;
+      A.vecs = idx->vecs;
+      A.perm_t = OT.perm;
+      A.perm_c = OC.perm;
+      A.ovf = ovf;
+      A.ovf_list = ovf_list;
+      A.ovf_count = ovf_count;
+      A.k = k;
+      A.kprime = kprime;
+      A.capb = capb;
+      A.seeded = seeded;
+      A.ids = d_ids;
+      A.dists = d_dists;
+      A.n_f64 = n_f64;
+      A.nbig_d = P.cnt + DP_NBIG;
+      uint32_t *spill = spill_count + 1;
+      k_merge_rerank<RR_CAP_SMALL><<<std::min<uint32_t>(nq, (uint32_t)idx->num_sms * 32), RR_THREADS,
+                                     sizeof(RerankSmem<RR_CAP_SMALL>), st>>>(A, 0, nullptr, nullptr, spill,
+                                                                             spill_count);
+      k_merge_rerank<RR_CAP><<<148 * 2, RR_THREADS, sizeof(RerankSmem<RR_CAP>), st>>>(A, 0, spill, spill_count,
+                                                                                       nullptr, nullptr);
+      g_launches += 2;
+      FKNN_CUDA(cudaEventRecord(G.ev[2], st));
+      if ((r = launch_exact_scan(idx, ovf_list, ovf_count, 0, 148 * 2, d_desc, d_q, k, d_ids, d_dists, st))) return r;
+      if ((r = launch_exact_scan(idx, P.small, P.cnt + DP_NSMALL, 0, 148 * 8, d_desc, d_q, k, d_ids, d_dists, st)))
+        return r;
+      FKNN_CUDA(cudaEventRecord(G.ev[3], st));
+      FKNN_CUDA(cudaGetLastError());
+      return FKNN_OK;
+    };
+    const int brc = body();
+    cudaGraph_t graph = nullptr;
+    const cudaError_t ce = cudaStreamEndCapture(st, &graph);
+    st = user_st;
+    if (brc || ce != cudaSuccess) {
+      if (graph) cudaGraphDestroy(graph);
+      G.release();
+      cudaGetLastError();
+      return brc ? brc : cuda_fail(ce, "cudaStreamEndCapture");
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&G.exec, graph, 0);
+    cudaGraphDestroy(graph);
+    if (ie != cudaSuccess) {
+      G.exec = nullptr;
+      G.release();
+      return cuda_fail(ie, "cudaGraphInstantiate");
+    }
+    G.key = key;
+    G.launches = g_launches - l0;
+    st = user_st;
+  }
+  g_launches = G.launches;
+  FKNN_CUDA(cudaGraphLaunch(G.exec, st));
+  int flag = 0;
+  FKNN_CUDA(cudaMemcpyAsync(&flag, idx->d_flag, sizeof(int), cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaStreamSynchronize(st));
+  if ((rc = check_query_flag_value(flag & ~ERR_WAIT_TIMEOUT))) return rc;
+  if (stats) {
+    float ms = 0.f;
+    FKNN_CUDA(cudaEventElapsedTime(&ms, G.ev[0], G.ev[1]));
+    stats->ms_screen = ms;
+    FKNN_CUDA(cudaEventElapsedTime(&ms, G.ev[1], G.ev[2]));
+    stats->ms_merge = ms;
+    FKNN_CUDA(cudaEventElapsedTime(&ms, G.ev[2], G.ev[3]));
+    stats->ms_scan = ms;
+    uint32_t c[16];
+    FKNN_CUDA(cudaMemcpy(c, P.cnt, sizeof(c), cudaMemcpyDeviceToHost));
+    uint32_t h2[2] = {0, 0};
+    FKNN_CUDA(cudaMemcpy(h2, d_state + 3 * (size_t)nq, 8, cudaMemcpyDeviceToHost));
+    auto u64 = [&](int i) { return (uint64_t)c[i] | ((uint64_t)c[i + 1] << 32); };
+    stats->pairs_screened = u64(10);
+    stats->pairs_passing = u64(12);
+    stats->pairs_contraction = u64(14);
+    stats->n_tiles = c[DP_NTILE];
+    stats->n_work_items = c[DP_NITEMS];
+    stats->n_small = c[DP_NSMALL];
+    stats->ms_plan = 0.f;
+    stats->n_overflow = h2[0];
+    stats->n_boundary_f64 = h2[1];
+  }
+  return FKNN_OK;
+}
+
 int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
                 uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
   return search_tc<FmtBF16>(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+}
+
+int search_bf16_graph(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k,
+                      uint32_t kprime, uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  return search_tc_graph<FmtBF16>(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+}
+
+int search_fp8_graph(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k,
+                     uint32_t kprime, uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats) {
+  return search_tc_graph<FmtFP8>(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
 }
 
 int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,

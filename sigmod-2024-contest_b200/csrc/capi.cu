@@ -89,6 +89,8 @@ static void free_index(fknn_index *idx) {
   if (!idx) return;
   cudaSetDevice(idx->device);
   cudaDeviceSynchronize();
+  idx->graph.release();
+  if (idx->graph.cap) cudaStreamDestroy(idx->graph.cap);
   if (idx->side_stream) cudaStreamDestroy(idx->side_stream);
   if (idx->ev_fork) cudaEventDestroy(idx->ev_fork);
   if (idx->ev_join) cudaEventDestroy(idx->ev_join);
@@ -143,6 +145,7 @@ int make_index_view(fknn_index *base, fknn_index **out) {
   v->fp8_scale = base->fp8_scale;
   for (int m = 0; m < 3; ++m) v->tuning[m] = base->tuning[m];
   v->num_sms = base->num_sms;
+  v->n_labels = base->n_labels;
   v->is_view = true;
   cudaError_t e = cudaSetDevice(v->device);
   if (e == cudaSuccess) e = cudaMalloc(&v->d_flag, 64);
@@ -305,6 +308,10 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     return FKNN_EINVAL;
   }
   const uint32_t kprime = (opts && opts->kprime) ? opts->kprime : 400;
+  if (opts && (opts->flags & ~FKNN_SEARCH_GRAPH)) {
+    set_error("fknn_search: unknown flag in fknn_search_opts.flags");
+    return FKNN_EINVAL;
+  }
   if (mode == FKNN_MODE_BF16_RERANK || mode == FKNN_MODE_FP8_RERANK) {
     if (mode == FKNN_MODE_BF16_RERANK ? !idx->bf16_blocks[0] : !idx->fp8_blocks[0]) {
       set_error(mode == FKNN_MODE_BF16_RERANK ? "fknn_search: BF16 mode needs an index created with build_bf16"
@@ -340,10 +347,11 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
     if ((rc = ws_get(idx, 8, (size_t)nq * k * 4, (void **)&d_ids))) return rc;
   if (dists && !dd_dev)
     if ((rc = ws_get(idx, 9, (size_t)nq * k * 4, (void **)&d_dists))) return rc;
+  const bool graph = opts && (opts->flags & FKNN_SEARCH_GRAPH);
   if (mode == FKNN_MODE_BF16_RERANK)
-    rc = search_bf16(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+    rc = (graph ? search_bf16_graph : search_bf16)(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
   else if (mode == FKNN_MODE_FP8_RERANK)
-    rc = search_fp8(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
+    rc = (graph ? search_fp8_graph : search_fp8)(idx, d_q, d_meta, nq, k, kprime, d_ids, d_dists, st, stats);
   else
     rc = search_exact(idx, d_q, d_meta, nq, k, d_ids, d_dists, st, stats);
   // on a failure the short-slab scans may still be writing the outputs

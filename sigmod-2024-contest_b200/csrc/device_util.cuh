@@ -17,6 +17,7 @@ constexpr int ERR_WAIT_TIMEOUT = 1 << 8;
 constexpr int ERR_BAD_QUERY_TYPE = 1 << 0;
 constexpr int ERR_BAD_QUERY_VALUE = 1 << 1;
 constexpr int ERR_BAD_QUERY_VEC = 1 << 2;
+constexpr int ERR_PLAN_BOUND = 1 << 3;  // a device-built plan met a buffer bound (reported, never written past)
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return (uint32_t)__cvta_generic_to_shared(p);
@@ -210,7 +211,8 @@ __device__ __forceinline__ int sq8_dist(const int *__restrict__ qw, int qq, cons
 // item counts (item_slot[item0 + i] selects the item, lane L of tq the
 // list) 32 at a time and scans them with shuffles.  prefix[i] = first
 // position of item i, *total = their sum, or over_value when there are more
-// than max_items items.  Caller: the whole block, then __syncthreads().
+// than max_items items (item_slot NULL: the items are item0 .. item0 +
+// nitems - 1).  Caller: the whole block, then __syncthreads().
 __device__ __forceinline__ void list_offsets(const uint32_t *__restrict__ item_slot, uint32_t item0, uint32_t nitems,
                                              const uint32_t *__restrict__ out_cnt, uint32_t L, uint32_t tq,
                                              uint32_t *prefix, int *total, uint32_t max_items, int over_value) {
@@ -223,7 +225,7 @@ __device__ __forceinline__ void list_offsets(const uint32_t *__restrict__ item_s
   uint32_t carry = 0;
   for (uint32_t base = 0; base < nitems; base += 32) {
     const uint32_t i = base + lane;
-    const uint32_t c = i < nitems ? out_cnt[(uint64_t)item_slot[item0 + i] * tq + L] : 0u;
+    const uint32_t c = i < nitems ? out_cnt[(uint64_t)(item_slot ? item_slot[item0 + i] : item0 + i) * tq + L] : 0u;
     uint32_t inc = c;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {

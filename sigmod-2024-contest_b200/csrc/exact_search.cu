@@ -307,7 +307,8 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
   }
 
   // ---------------- consumers
-  bool ok = mbar_wait_bounded(&sm.qbar, 0, err);
+  // waits are warp-uniform: the lanes' timers may disagree at the deadline
+  bool ok = __all_sync(0xffffffffu, mbar_wait_bounded(&sm.qbar, 0, err));
   if (lane < 16) {
     const int L = 16 * warp + lane;
     const int32_t qi = lane_q[it.tile * TQ + L];
@@ -333,7 +334,7 @@ __global__ void __launch_bounds__(SC_THREADS, 2)
   const int tx = tid >> 4;  // queries tx*8 .. tx*8+7 of the tile (owned by this warp)
   for (uint32_t sub = 0; sub < nsub && ok; ++sub) {
     const int st = sub % SC_STAGES;
-    if (!mbar_wait_bounded(&sm.full[st], (sub / SC_STAGES) & 1, err)) {
+    if (!__all_sync(0xffffffffu, mbar_wait_bounded(&sm.full[st], (sub / SC_STAGES) & 1, err))) {
       ok = false;
       break;
     }
@@ -772,6 +773,10 @@ int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uin
 
 static int check_query_flag(int flag) {
   if (!flag) return FKNN_OK;
+  if (flag == ERR_PLAN_BOUND) {
+    set_error("fknn_search: the device-built plan met a buffer bound (internal error; no output was written past it)");
+    return FKNN_ECUDA;
+  }
   std::string m = "fknn_search: ";
   if (flag & ERR_BAD_QUERY_TYPE) m += "query type not in {0,1,2,3}; ";
   if (flag & ERR_BAD_QUERY_VALUE) m += "query category outside int32 or NaN window bound; ";
@@ -1020,6 +1025,19 @@ void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint6
   }
   P.items.swap(items);
 }
+
+int enqueue_query_prep(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, QueryDesc *d_desc,
+                       cudaStream_t st) {
+  int rc;
+  if ((rc = validate_queries(idx, d_q, d_meta, nq, st))) return rc;
+  k_query_prep<<<(nq + 255) / 256, 256, 0, st>>>(d_q, d_meta, nq, (uint32_t)idx->n, idx->ord[ORDER_TIME].ts,
+                                                 idx->ord[ORDER_CAT].label, idx->ord[ORDER_CAT].ts, d_desc);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int check_query_flag_value(int flag) { return check_query_flag(flag); }
 
 int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,
                     QueryDesc **d_desc_out, QueryDesc **h_desc_out, float **h_meta_out) {

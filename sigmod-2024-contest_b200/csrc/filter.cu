@@ -4,23 +4,22 @@
 // predicate's passing row ids in increasing order.
 //
 // One pass over the columns for up to FP_MAXP predicates (k_filter_scan,
-// a single-pass scan with decoupled look-back):
+// a single-pass scan):
 //   * a CTA takes the next 4,096-row tile from a ticket counter, so every
 //     tile before it is already running or done;
 //   * its threads load the tile's labels and timestamps as float4 (16 rows
 //     each, coalesced) and evaluate every predicate on them;
-//   * per predicate the tile's passing count is published at once (flag
-//     AGGREGATE), the prefix of the tiles before it is read from their
-//     published words (one warp looks back 32 tiles at a time and stops at
-//     the nearest INCLUSIVE one), the tile's inclusive prefix is published,
-//     and every passing row writes its id at prefix + its rank in the tile.
+//   * per predicate the tile publishes its passing count at once, then sums
+//     the counts of all the tiles before it (each thread a strided share, so
+//     no tile waits on another tile's prefix: only on counts published
+//     right after their loads), and every passing row writes its id at
+//     prefix + its rank in the tile.
 // A status word holds its flag and its value together, so one 64-bit
-// volatile load sees a consistent pair.  The waits on predecessors are
-// bounded by the global timer; a look-back that gives up marks its tile, so
-// the tiles after it give up too, and that predicate's count is UINT64_MAX.
-// Nothing is read back: the counts land in device memory, so a batch of
-// calls streams back to back.  Algorithmic traffic per launch: 8 B per row
-// plus 4 B per passing row.
+// volatile load sees a consistent pair.  The waits are bounded by the
+// global timer; a tile that gives up makes that predicate's count
+// UINT64_MAX.  Nothing is read back: the counts land in device memory, so
+// a batch of calls streams back to back.  Algorithmic traffic per launch:
+// 8 B per row plus 4 B per passing row.
 #include <algorithm>
 #include <cstring>
 
@@ -36,8 +35,8 @@ constexpr int FS_IT = 4;                          // float4 loads per column per
 constexpr int FS_TILE = FS_THREADS * 4 * FS_IT;   // 4,096 rows per tile
 constexpr int FS_SEG = FS_IT * FS_NW;             // 128-row warp segments per tile (= 32)
 constexpr uint32_t FP_MAXP = 16;                  // predicates per launch
-constexpr uint64_t ST_AGG = 1ull << 62, ST_INC = 2ull << 62, ST_FLAGS = 3ull << 62;
-constexpr uint64_t ST_BAD = 1ull << 61;  // a tile whose look-back gave up: its successors give up too
+constexpr uint64_t ST_AGG = 1ull << 62, ST_FLAGS = 3ull << 62;
+constexpr uint32_t FS_UNROLL = 4;                 // status words in flight per thread
 
 static_assert(FS_SEG == 32, "one warp scans the tile's segments");
 
@@ -68,8 +67,9 @@ __global__ void __launch_bounds__(FS_THREADS) k_filter_scan(const float *__restr
                                                             uint64_t *__restrict__ counts) {
   __shared__ float4 pm[FP_MAXP];
   __shared__ uint32_t seg[FS_SEG];
-  __shared__ uint32_t s_tile;
-  __shared__ uint64_t s_prefix;
+  __shared__ uint32_t s_tile, s_total;
+  __shared__ uint64_t s_prefix, s_part[FS_NW];
+  __shared__ int s_fail[FS_NW];
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   if (tid < (int)FP_MAXP) pm[tid] = P.m[tid];
   if (tid == 0) s_tile = atomicAdd(ticket, 1u);
@@ -131,6 +131,7 @@ __global__ void __launch_bounds__(FS_THREADS) k_filter_scan(const float *__restr
       if (lane == 31) seg[it * FS_NW + w] = inc;
     }
     __syncthreads();
+    uint64_t *st = status + (uint64_t)p * ntiles;
     if (w == 0) {
       // the 32 segments in row order (it-major, then warp): exclusive offsets
       const uint32_t v = seg[lane];
@@ -141,55 +142,55 @@ __global__ void __launch_bounds__(FS_THREADS) k_filter_scan(const float *__restr
         if (lane >= o) inc += x;
       }
       seg[lane] = inc - v;
-      const uint32_t total = __shfl_sync(0xffffffffu, inc, 31);
-      uint64_t *st = status + (uint64_t)p * ntiles;
-      uint64_t prefix = 0;
-      bool failed = false;
-      if (t > 0) {
-        if (lane == 0) {
-          __threadfence();
-          *(volatile uint64_t *)(st + t) = ST_AGG | total;
-        }
-        // look back 32 tiles at a time, down to the nearest tile that has
-        // published its inclusive prefix (before tile 0 the prefix is 0)
-        int64_t j = (int64_t)t - 1;
-        const uint64_t t0 = global_ns();
-        while (j >= 0) {
-          const int64_t jj = j - lane;
-          uint64_t sv = jj >= 0 ? ld_volatile_u64(st + jj) : ST_INC;
-          // every predecessor publishes its aggregate without waiting on
-          // anything, so these waits end; they are bounded all the same
-          // (every vote below is taken by all 32 lanes: the loop exits together)
-          while (true) {
-            const bool pending = (sv & ST_FLAGS) == 0;
-            if (!__any_sync(0xffffffffu, pending)) break;
-            if (__any_sync(0xffffffffu, global_ns() - t0 > WAIT_NS)) {
-              failed = true;
-              break;
-            }
-            if (pending) sv = ld_volatile_u64(st + jj);
-          }
-          if (failed) break;
-          const uint32_t inc_lanes = __ballot_sync(0xffffffffu, (sv & ST_FLAGS) == ST_INC);
-          const int stop = inc_lanes ? __ffs(inc_lanes) - 1 : 31;
-          if (__any_sync(0xffffffffu, lane <= stop && (sv & ST_BAD))) {
-            failed = true;
-            break;
-          }
-          uint64_t val = (lane <= stop && jj >= 0) ? (sv & 0xffffffffull) : 0ull;
+      if (lane == 31) {
+        s_total = inc;
+        *(volatile uint64_t *)(st + t) = ST_AGG | inc;  // published before this tile waits on anything
+      }
+    }
+    // the tile's prefix: every thread sums a strided share of the counts the
+    // tiles before it published (they took their tickets first, so they run
+    // and publish without waiting); the waits are bounded
+    uint64_t part = 0;
+    bool failed = false;
+    const uint64_t t0 = global_ns();
+    for (uint32_t j0 = tid; j0 < t && !failed; j0 += FS_UNROLL * FS_THREADS) {
+      uint64_t sv[FS_UNROLL];
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-          prefix += val;
-          if (inc_lanes) break;
-          j -= 32;
+      for (uint32_t u = 0; u < FS_UNROLL; ++u) {
+        const uint32_t j = j0 + u * FS_THREADS;
+        sv[u] = j < t ? ld_volatile_u64(st + j) : ST_AGG;  // independent loads, in flight together
+      }
+#pragma unroll
+      for (uint32_t u = 0; u < FS_UNROLL; ++u) {
+        while (!failed && (sv[u] & ST_FLAGS) == 0) {
+          if (global_ns() - t0 > WAIT_NS) failed = true;
+          else sv[u] = ld_volatile_u64(st + j0 + u * FS_THREADS);
         }
+        part += sv[u] & 0xffffffffull;
       }
-      if (lane == 0) {
-        __threadfence();
-        *(volatile uint64_t *)(st + t) = failed ? (ST_INC | ST_BAD) : (ST_INC | ((prefix + total) & 0xffffffffull));
-        s_prefix = failed ? ~0ull : prefix;
-        if (t == ntiles - 1) counts[p] = failed ? ~0ull : prefix + total;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    const uint32_t anyfail = __ballot_sync(0xffffffffu, failed);
+    if (lane == 0) {
+      s_part[w] = part;
+      s_fail[w] = anyfail ? 1 : 0;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      uint64_t pre = 0;
+      int f = 0;
+#pragma unroll
+      for (int j = 0; j < FS_NW; ++j) {
+        pre += s_part[j];
+        f |= s_fail[j];
       }
+      s_prefix = f ? ~0ull : pre;
+      // the count: the last tile's prefix plus its own; a tile that gave up
+      // raises it to UINT64_MAX (counts start at 0, combined by max)
+      unsigned long long *cp = reinterpret_cast<unsigned long long *>(counts + p);
+      if (f) atomicMax(cp, ~0ull);
+      else if (t == ntiles - 1) atomicMax(cp, (unsigned long long)(pre + s_total));
     }
     __syncthreads();
     const uint64_t prefix = s_prefix;
@@ -249,6 +250,7 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
     }
     uint32_t *ticket = reinterpret_cast<uint32_t *>(status + (size_t)m * ntiles);
     FKNN_CUDA(cudaMemsetAsync(status, 0, ((size_t)m * ntiles + 1) * sizeof(uint64_t), st));
+    FKNN_CUDA(cudaMemsetAsync(d_counts + p0, 0, (size_t)m * sizeof(uint64_t), st));
     k_filter_scan<<<ntiles, FS_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, P, m, ntiles, status, ticket,
                                                  d_out + (uint64_t)p0 * n, n, d_counts + p0);
     g_launches += 1;

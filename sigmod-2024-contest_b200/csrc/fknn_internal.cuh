@@ -168,12 +168,52 @@ struct PlanShape {
 void make_plan(const QueryDesc *desc, const float *meta_host, uint32_t nq, uint64_t n, const PlanShape &shape,
                Plan &P);
 
+// A search plan built on the device (device_plan.cu), for captured searches:
+// the same tiles / work items as Plan, laid out in one device buffer, with
+// every count in device memory (cnt).
+struct DevPlanSizes {
+  uint64_t nb_all = 1;   // start buckets
+  uint32_t bw = 1;       // bucket width in rows
+  uint32_t ntile_max = 1, nitems_max = 1;
+};
+struct DevPlan {
+  uint32_t nq = 0;
+  DevPlanSizes z;
+  uint32_t *cnt = nullptr;  // [0] big queries, [1] small, [2] tiles, [3] items, [8..15] 64-bit pair counts
+  uint32_t *key_lo = nullptr, *key_hi = nullptr, *vals = nullptr, *ktmp = nullptr, *vtmp = nullptr;
+  uint32_t *seg = nullptr, *lane = nullptr, *tflag = nullptr;
+  uint32_t *big_q = nullptr, *big_tile = nullptr, *big_lane = nullptr, *small = nullptr;
+  uint32_t *tile_first = nullptr, *tS = nullptr, *tE = nullptr, *nblk = nullptr, *chunk = nullptr, *nit = nullptr;
+  uint32_t *spare = nullptr, *bsum = nullptr;
+  Tile *tiles = nullptr;
+  WorkItem *items = nullptr;
+};
+constexpr int DP_NBIG = 0, DP_NSMALL = 1, DP_NTILE = 2, DP_NITEMS = 3;
+
 // Device data of one row order.
 struct OrderData {
   float *blocks = nullptr;     // [nblk][101][64]
   uint32_t *perm = nullptr;    // [n] position -> row id
   float *ts = nullptr;         // [n] timestamps in this order
   int32_t *label = nullptr;    // [n] int32 labels in this order
+};
+
+// A captured search (BF16 / FP8 with a device plan): replayed while the
+// call's shape, pointers and scratch buffers stay the same.
+struct GraphCache {
+  cudaGraphExec_t exec = nullptr;
+  std::vector<uint64_t> key;
+  uint32_t launches = 0;   // kernels in the graph
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // screen / merge / scan boundaries
+  cudaStream_t cap = nullptr;  // the capture runs here: the caller's stream may be the legacy one
+  void release() {
+    if (exec) cudaGraphExecDestroy(exec);
+    exec = nullptr;
+    key.clear();
+    for (auto &e : ev)
+      if (e) cudaEventDestroy(e);
+    for (auto &e : ev) e = nullptr;
+  }
 };
 
 // Grow-only device arena for per-call scratch.
@@ -206,7 +246,7 @@ struct fknn_index {
   float *fp8_scale = nullptr;
   // per-call scratch
   std::mutex mu;
-  fknn::DevBuf ws[19];
+  fknn::DevBuf ws[20];
   fknn::HostBuf hs[8];
   int *d_flag = nullptr;
   cudaStream_t own_stream = nullptr;
@@ -217,11 +257,14 @@ struct fknn_index {
   // per-mode plan / kernel parameters (fknn_index_set_tuning) and the SM count
   fknn_tuning tuning[3] = {{0, 16, 16, 0, 0}, {256, 3, 8, 0, 16}, {256, 3, 8, 0, 16}};
   int num_sms = 148;
+  uint32_t n_labels = 1;  // distinct category values (bounds a device plan's segments)
   // a view shares the device data of another index and owns only its
   // per-call scratch (ws, hs, d_flag), so views search concurrently
   bool is_view = false;
   // test hook: the next reduced-precision search withholds one row-block copy
   bool test_withhold = false;
+  // captured searches (fknn_search_opts.flags & FKNN_SEARCH_CAPTURE)
+  fknn::GraphCache graph;
 };
 
 namespace fknn {
@@ -255,6 +298,13 @@ int build_index_from_columns(fknn_index *idx, cudaStream_t st);
 int radix_sort_pairs(fknn_index *idx, uint32_t *keys, uint32_t *vals, uint32_t *keys_tmp, uint32_t *vals_tmp,
                      uint64_t n, int begin_bit, int end_bit, cudaStream_t st);
 
+// device-built plans (device_plan.cu)
+DevPlanSizes device_plan_sizes(const fknn_index *idx, uint32_t nq, const PlanShape &shape);
+size_t device_plan_bytes(uint32_t nq, const DevPlanSizes &z);
+void device_plan_layout(DevPlan &P, void *mem, uint32_t nq, const DevPlanSizes &z);
+int device_plan_build(fknn_index *idx, const QueryDesc *d_desc, const float *d_meta, DevPlan &P,
+                      const PlanShape &shape, cudaStream_t st);
+
 // exact search (exact_search.cu)
 int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
                  float *d_dists, cudaStream_t st, fknn_search_stats *stats);
@@ -265,6 +315,10 @@ int filter_rows_batch(fknn_index *idx, const float *metas_host, uint32_t np, uin
                       cudaStream_t st);
 int filter_rows(fknn_index *idx, const float *meta4_host, uint32_t *d_out, uint64_t *count, cudaStream_t st);
 int validate_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st);
+// validation flag cleared and set, and the query descriptors, enqueued only
+int enqueue_query_prep(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, QueryDesc *d_desc,
+                       cudaStream_t st);
+int check_query_flag_value(int flag);
 int prepare_queries(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, cudaStream_t st,
                     QueryDesc **d_desc, QueryDesc **h_desc, float **h_meta);
 int launch_exact_scan(fknn_index *idx, const uint32_t *list, const uint32_t *d_count, uint32_t h_count, unsigned grid,
@@ -282,6 +336,11 @@ int search_fp8(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t 
                uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 int search_bf16(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t kprime,
                 uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
+// the same with the plan built on the device and the whole search one captured CUDA graph
+int search_bf16_graph(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k,
+                      uint32_t kprime, uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
+int search_fp8_graph(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k,
+                     uint32_t kprime, uint32_t *d_ids, float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 
 // FP32 re-rank of device candidate lists, no synchronisation (rerank.cu)
 int launch_rerank(fknn_index *idx, const float *d_q, uint32_t nq, const uint32_t *d_cand, uint32_t nc, uint32_t k,

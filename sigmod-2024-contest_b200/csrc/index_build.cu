@@ -190,6 +190,14 @@ __global__ void k_build_blocks(const float *__restrict__ vecs, const float *__re
   }
 }
 
+// distinct labels: starts of the label runs of the category order
+__global__ void k_label_runs(const int32_t *__restrict__ lab, uint64_t n, uint32_t *__restrict__ count) {
+  uint32_t c = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+    c += (i == 0 || lab[i] != lab[i - 1]) ? 1u : 0u;
+  if (c) atomicAdd(count, c);
+}
+
 inline unsigned grid_for(uint64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
 
 }  // namespace
@@ -285,8 +293,14 @@ int build_index_from_columns(fknn_index *idx, cudaStream_t st) {
     k_build_blocks<<<idx->nblk, 256, 0, st>>>(idx->vecs, idx->norms, od.perm, n, od.blocks);
     g_launches += 2;
   }
+  FKNN_CUDA(cudaMemsetAsync(idx->d_flag, 0, sizeof(int), st));
+  k_label_runs<<<148 * 4, 256, 0, st>>>(idx->ord[ORDER_CAT].label, n, reinterpret_cast<uint32_t *>(idx->d_flag));
+  g_launches += 1;
   FKNN_CUDA(cudaGetLastError());
+  uint32_t runs = 0;
+  FKNN_CUDA(cudaMemcpyAsync(&runs, idx->d_flag, 4, cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
+  idx->n_labels = runs ? runs : 1;
   return FKNN_OK;
 }
 

@@ -412,7 +412,8 @@ __global__ void __launch_bounds__(SQ_THREADS, 2)
     bool ok = true;
     for (uint32_t sub = 0; sub < ntile; ++sub) {
       const int ab = sub & 1;
-      if (!mbar_wait_bounded(&sm.accfull[ab], (sub >> 1) & 1, err)) {
+      // warp-uniform: the lanes' timers may disagree at the deadline
+      if (!__all_sync(0xffffffffu, mbar_wait_bounded(&sm.accfull[ab], (sub >> 1) & 1, err))) {
         ok = false;
         break;
       }

@@ -25,6 +25,7 @@ FKNN_ENODEV = -6
 MODE_EXACT_FP32 = 0
 MODE_BF16_RERANK = 1
 MODE_FP8_RERANK = 2
+SEARCH_GRAPH = 1  # fknn_search_opts.flags FKNN_SEARCH_GRAPH
 
 # Graph search forms (include/fknn.h FKNN_GRAPH_*), numbered as the Searcher methods.
 GRAPH_SEARCH = 0
@@ -63,7 +64,7 @@ class Tuning(Structure):
 
 
 class SearchOpts(Structure):
-    _fields_ = [("mode", c_int), ("kprime", c_uint32)]
+    _fields_ = [("mode", c_int), ("kprime", c_uint32), ("flags", c_uint32)]
 
 
 class SearchStats(Structure):

@@ -24,7 +24,7 @@ from typing import Optional, Sequence
 import numpy as np
 
 from . import _lib
-from ._lib import (MODE_BF16_RERANK, MODE_EXACT_FP32, MODE_FP8_RERANK, IndexOpts, SearchOpts, SearchStats,
+from ._lib import (MODE_BF16_RERANK, MODE_EXACT_FP32, MODE_FP8_RERANK, SEARCH_GRAPH, IndexOpts, SearchOpts, SearchStats,
                    ServerOpts, ServerStats, Tuning, check, load)
 
 DIM = 100
@@ -127,11 +127,14 @@ class Index:
         return b.value
 
     def search(self, qvecs, metas, k: int = K, mode: int = MODE_EXACT_FP32, ids=None, dists=None,
-               kprime: int = 0, with_dists: bool = True, stream: Optional[int] = None, return_stats: bool = False):
+               kprime: int = 0, with_dists: bool = True, stream: Optional[int] = None, return_stats: bool = False,
+               graph: bool = False):
         """Filtered top-k.  metas rows are (type, v, l, r) as in utils.h:98-101.
 
         Returns (ids, dists) as numpy arrays for host inputs, or the given /
-        newly allocated torch CUDA tensors for device inputs.
+        newly allocated torch CUDA tensors for device inputs.  graph=True
+        (reduced-precision modes) plans on the device and replays a captured
+        CUDA graph while nq, k, kprime, the tuning and the buffers repeat.
         """
         lib = load()
         dev = _is_torch(qvecs) and qvecs.is_cuda
@@ -148,7 +151,7 @@ class Index:
                 dists = np.empty((nq, k), dtype=np.float32) if with_dists else None
         if stream is None:
             stream = _stream_of(qvecs, metas, ids)
-        opts = SearchOpts(mode, kprime)
+        opts = SearchOpts(mode, kprime, SEARCH_GRAPH if graph else 0)
         st = SearchStats()
         check(lib.fknn_search_ex(self._h, _ptr(qvecs, np.float32), _ptr(metas, np.float32), nq, k, byref(opts),
                                  _ptr(ids, np.uint32), _ptr(dists, np.float32) if dists is not None else None,

@@ -28,9 +28,10 @@ DEFAULT_TABLE = os.path.join(os.path.dirname(os.path.abspath(__file__)), "tuning
 
 SPACE = {
     "items_per_sm": [2, 3, 4, 6, 8],
-    "pilot_stride": [0, 8, 16, 32],
+    "pilot_stride": [0, 8, 16, 32, 64],
     "list_slack": [256, 384, 512],
     "min_chunk_blocks": [4, 8, 16],
+    "bound_refresh": [0, 2, 8, 32],
 }
 EXACT_SPACE = {"items_per_sm": [8, 12, 16, 24], "min_chunk_blocks": [8, 16, 32], "pilot_stride": [0, 8, 16, 32]}
 KPRIMES = [100, 112, 128, 160, 200, 256, 320, 400, 512, 640, 800, 1024]
