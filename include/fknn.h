@@ -370,6 +370,10 @@ typedef struct fknn_router_stats {
   uint32_t n_bruteforce, n_category, n_type0, n_type2;  /* queries per route */
   uint32_t n_graph_calls, n_split_small, n_split_medium, n_split_full;
   float ms_total;            /* wall time of the call */
+  /* wall time of each stage (each ends with its results on the host or in
+   * the output): query upload + slabs, SQ8 brute force + re-rank, category
+   * graphs + re-rank, type-0 buckets, type-2 splits, pooled re-rank + copy-out */
+  float ms_prepare, ms_bruteforce, ms_category, ms_type0, ms_type2, ms_final;
 } fknn_router_stats;
 
 int fknn_router_default_params(fknn_router_params *p);

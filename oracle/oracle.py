@@ -208,7 +208,7 @@ def ref_graph() -> ctypes.CDLL | None:
         L.ref_hnsw_build.argtypes = [c_void_p, c_void_p, c_int, c_int, c_int, ctypes.c_char_p]
         L.ref_graph_search.restype = c_int
         L.ref_graph_search.argtypes = [ctypes.c_char_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int,
-                                       c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p]
+                                       c_int, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]
         _rg = L
     return _rg
 
@@ -255,8 +255,10 @@ def ref_hnsw_graph(vecs, ts, R: int, efc: int, path: str) -> bytes:
 
 
 def ref_graph_search(path: str, vecs, labels, ts, queries, mode: int, k: int, refine: int, bounds=None,
-                     id_bounds=None, with_dists: bool = False):
-    """The reference Searcher itself over the graph saved at path."""
+                     id_bounds=None, with_dists: bool = False, timing: list | None = None):
+    """The reference Searcher itself over the graph saved at path.  timing:
+    a list that receives the seconds of the query loop alone (graph load and
+    SetData excluded)."""
     R_ = ref_graph()
     if R_ is None:
         raise RuntimeError("oracle/_ref/libref_graph.so is not built")
@@ -267,11 +269,14 @@ def ref_graph_search(path: str, vecs, labels, ts, queries, mode: int, k: int, re
     ib, ibp = _opt_ptr(id_bounds, np.int32, (nq, 2))
     ids = np.empty((nq, refine), dtype=np.int32)
     d = np.empty((nq, refine), dtype=np.float32) if with_dists else None
+    secs = ctypes.c_double(0.0)
     rc = R_.ref_graph_search(path.encode(), vecs.ctypes.data, labels.ctypes.data, ts.ctypes.data, vecs.shape[0],
                              q.ctypes.data, nq, mode, k, refine, bp, ibp, ids.ctypes.data,
-                             d.ctypes.data if with_dists else None)
+                             d.ctypes.data if with_dists else None, ctypes.byref(secs))
     if rc != 0:
         raise RuntimeError("ref_graph_search failed")
+    if timing is not None:
+        timing.append(secs.value)
     return (ids, d) if with_dists else ids
 
 

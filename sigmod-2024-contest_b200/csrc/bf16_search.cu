@@ -324,6 +324,7 @@ struct BScreenSmem {
   float stage[B_EPI_WARPS][32 * STAGE_ROW];
   uint64_t full[BS], empty[BS], accfull[2], accempty[2], abar;
   uint32_t tmem_base;
+  uint32_t next[2];  // the next processing slot, by item parity (work queue)
 };
 
 // two screening CTAs share an SM (228 KB of shared memory, 1 KB reserved per CTA)
@@ -494,7 +495,8 @@ __global__ void __launch_bounds__(B_THREADS, 2)
                 const unsigned char *__restrict__ blocks_t, const unsigned char *__restrict__ blocks_c,
                 uint32_t *__restrict__ T_global, uint32_t *__restrict__ ovf, Candidate *__restrict__ out,
                 uint32_t *__restrict__ out_cnt, uint32_t kprime, uint32_t capb, uint32_t refresh, uint32_t stride,
-                uint32_t withhold, uint32_t nitems_h, const uint32_t *__restrict__ nitems_d, int *err) {
+                uint32_t withhold, uint32_t nitems_h, const uint32_t *__restrict__ nitems_d,
+                const uint32_t *__restrict__ order, uint32_t *queue, int *err) {
   extern __shared__ __align__(1024) unsigned char smem_raw[];
   BScreenSmem<F> &sm = *reinterpret_cast<BScreenSmem<F> *>(smem_raw);
   constexpr uint32_t TB = Tiles<F>::BYTES;
@@ -529,7 +531,11 @@ __global__ void __launch_bounds__(B_THREADS, 2)
   // a bounded wait gave up: the CTA's later items only mark their queries
   // (combined over the block at each item's closing barrier, so uniform)
   bool aborted = false;
-  for (uint32_t item_id = blockIdx.x; item_id < nitems; item_id += gridDim.x, ++iter) {
+  // processing slots: blockIdx.x first, then the next free slot of the work
+  // queue (queue != NULL) or blockIdx.x + k * gridDim.x; slot -> item
+  // through order (longest first) when given
+  for (uint32_t slot = blockIdx.x; slot < nitems; ++iter) {
+    const uint32_t item_id = order ? order[slot] : slot;
     const WorkItem it = items[item_id];
     const Tile tl = tiles[it.tile];
     const unsigned char *blocks = tl.order == ORDER_TIME ? blocks_t : blocks_c;
@@ -697,10 +703,14 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       }
     }
     g += nsub;
+    // double-buffered by item parity: a slow thread may still read the slot
+    // of this barrier while thread 0 writes the one after
+    if (queue && tid == 0) sm.next[(iter + 1) & 1] = atomicAdd(queue, 1u) + gridDim.x;
     tc_fence_before();
     // the item's shared state (A tile, lists' counts, bounds) is reused by the next
     aborted = __syncthreads_or(aborted || gave_up) != 0;
     tc_fence_after();
+    slot = queue ? sm.next[(iter + 1) & 1] : slot + gridDim.x;
   }
   if (warp == 1) asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(TMEM_COLS));
 }
@@ -784,7 +794,7 @@ __device__ void merge_one(const MergeArgs &A, uint32_t b, RerankSmem<CAP> &sm, u
   }
   // the whole block copies each item's list
   for (uint32_t i = 0; i < nitems; ++i) {
-    const uint64_t item = item_slot[tl.item0 + i];
+    const uint64_t item = item_slot ? item_slot[tl.item0 + i] : tl.item0 + i;
     const uint32_t base = sm.cnt_prefix[i];
     const uint32_t c = (i + 1 < nitems ? sm.cnt_prefix[i + 1] : (uint32_t)M) - base;
     const Candidate *src = out + (item * BQ + L) * capb;
@@ -1069,7 +1079,7 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
       screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
           (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, ls, d_lqs,
           (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A, d_out,
-          d_ocnt, r, capb, 0, stride, 0u, nitems, nullptr, idx->d_flag);
+          d_ocnt, r, capb, 0, stride, 0u, nitems, nullptr, nullptr, nullptr, idx->d_flag);
       k_seed_bounds<<<std::max<uint32_t>(1, std::min<uint32_t>((nbig + 255) / 256, 1184)), 256, 0, st>>>(
           (const uint32_t *)(d_blob + o_big), nbig, nullptr, d_desc, T_A, ovf_A, 16 * stride * BR, T_global, seeded);
       g_launches += 3;
@@ -1077,7 +1087,8 @@ static int search_tc(fknn_index *idx, const float *d_q, const float *d_meta, uin
     screen<<<nitems, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
         (const WorkItem *)(d_blob + o_items), (const Tile *)(d_blob + o_tiles), d_at, ls, d_lqs,
         (const unsigned char *)blocks[ORDER_TIME], (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out,
-        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->test_withhold ? 1u : 0u, nitems, nullptr, idx->d_flag);
+        d_ocnt, kprime, capb, tune.bound_refresh, 1, idx->test_withhold ? 1u : 0u, nitems, nullptr, nullptr, nullptr,
+        idx->d_flag);
     idx->test_withhold = false;
     if (stats) FKNN_CUDA(cudaEventRecord(ev[1], st));
     MergeArgs A;
@@ -1188,7 +1199,8 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
   if (stride > 1 && (rc = ws_get(idx, 11, (size_t)nq * 12, (void **)&d_pilot))) return rc;
   {  // the radix sort's histogram slot at its largest (the plan sorts nq keys)
     void *h;
-    if ((rc = ws_get(idx, 15, ((size_t)(nq + 4095) / 4096) * 256 * sizeof(uint32_t) + 256, &h))) return rc;
+    const size_t keys = std::max<size_t>(nq, z.nitems_max);  // ... and the work items
+    if ((rc = ws_get(idx, 15, ((keys + 4095) / 4096) * 256 * sizeof(uint32_t) + 256, &h))) return rc;
   }
   DevPlan P;
   device_plan_layout(P, d_plan, nq, z);
@@ -1213,6 +1225,9 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
     G.release();
     for (auto &e : G.ev) FKNN_CUDA(cudaEventCreate(&e));
     if (!G.cap) FKNN_CUDA(cudaStreamCreateWithFlags(&G.cap, cudaStreamNonBlocking));
+    if (!G.side) FKNN_CUDA(cudaStreamCreateWithFlags(&G.side, cudaStreamNonBlocking));
+    if (!G.fork) FKNN_CUDA(cudaEventCreateWithFlags(&G.fork, cudaEventDisableTiming));
+    if (!G.join) FKNN_CUDA(cudaEventCreateWithFlags(&G.join, cudaEventDisableTiming));
     const uint32_t l0 = g_launches;
     const cudaStream_t user_st = st;
     st = G.cap;  // captured nodes carry no stream: the replay goes to the caller's
@@ -1222,6 +1237,15 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
       int r;
       if ((r = enqueue_query_prep(idx, d_q, d_meta, nq, d_desc, st))) return r;
       if ((r = device_plan_build(idx, d_desc, d_meta, P, shape, st))) return r;
+      // the short-slab exact scans need only the plan's list: a branch of
+      // the graph beside the contraction (their rows of ids / dists are
+      // disjoint from the merge's)
+      FKNN_CUDA(cudaEventRecord(G.fork, st));
+      FKNN_CUDA(cudaStreamWaitEvent(G.side, G.fork, 0));
+      if ((r = launch_exact_scan(idx, P.small, P.cnt + DP_NSMALL, 0, 148 * 8, d_desc, d_q, k, d_ids, d_dists,
+                                 G.side)))
+        return r;
+      FKNN_CUDA(cudaEventRecord(G.join, G.side));
       uint32_t *T_global = d_state, *ovf = d_state + nq, *ovf_list = d_state + 2 * (size_t)nq,
                *ovf_count = d_state + 3 * (size_t)nq, *n_f64 = ovf_count + 1, *spill_count = ovf_count + 2;
       if ((r = launch_fill_u32(T_global, nq, f32_sortable(INFINITY), st))) return r;
@@ -1240,7 +1264,7 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
       else
         k_tile_stage_bf16<<<tgrid, 256, 0, st>>>(d_q, ls, P.tiles, 0, d_desc, (__nv_bfloat16 *)d_at, d_lqs);
       g_launches += 1;
-      FKNN_CUDA(cudaEventRecord(G.ev[0], st));
+      FKNN_CUDA(cudaEventRecordWithFlags(G.ev[0], st, cudaEventRecordExternal));  // an event node of the graph
       void *const *blocks = F::kFP8 ? idx->fp8_blocks : idx->bf16_blocks;
       const unsigned sgrid = std::min<uint32_t>(z.nitems_max, (uint32_t)idx->num_sms * 2);
       uint32_t *seeded = nullptr;
@@ -1254,7 +1278,7 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
         screen<<<sgrid, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
             P.items, P.tiles, d_at, ls, d_lqs, (const unsigned char *)blocks[ORDER_TIME],
             (const unsigned char *)blocks[ORDER_CAT], T_A, ovf_A, d_out, d_ocnt, rr, capb, 0, stride, 0u, 0,
-            P.cnt + DP_NITEMS, idx->d_flag);
+            P.cnt + DP_NITEMS, P.ord_val, P.queue, idx->d_flag);
         k_seed_bounds<<<1184, 256, 0, st>>>(P.big_q, 0, P.cnt + DP_NBIG, d_desc, T_A, ovf_A, 16 * stride * BR,
                                             T_global, seeded);
         g_launches += 2;
@@ -1262,9 +1286,9 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
       screen<<<sgrid, B_THREADS, sizeof(BScreenSmem<F>), st>>>(
           P.items, P.tiles, d_at, ls, d_lqs, (const unsigned char *)blocks[ORDER_TIME],
           (const unsigned char *)blocks[ORDER_CAT], T_global, ovf, d_out, d_ocnt, kprime, capb, tune.bound_refresh, 1,
-          withhold ? 1u : 0u, 0, P.cnt + DP_NITEMS, idx->d_flag);
+          withhold ? 1u : 0u, 0, P.cnt + DP_NITEMS, P.ord_val, P.queue + 1, idx->d_flag);
       g_launches += 1;
-      FKNN_CUDA(cudaEventRecord(G.ev[1], st));
+      FKNN_CUDA(cudaEventRecordWithFlags(G.ev[1], st, cudaEventRecordExternal));  // an event node of the graph
       MergeArgs A;
       A.big_q = P.big_q;
       A.big_tile = P.big_tile;
@@ -1296,11 +1320,10 @@ static int search_tc_graph(fknn_index *idx, const float *d_q, const float *d_met
       k_merge_rerank<RR_CAP><<<148 * 2, RR_THREADS, sizeof(RerankSmem<RR_CAP>), st>>>(A, 0, spill, spill_count,
                                                                                        nullptr, nullptr);
       g_launches += 2;
-      FKNN_CUDA(cudaEventRecord(G.ev[2], st));
+      FKNN_CUDA(cudaEventRecordWithFlags(G.ev[2], st, cudaEventRecordExternal));  // an event node of the graph
       if ((r = launch_exact_scan(idx, ovf_list, ovf_count, 0, 148 * 2, d_desc, d_q, k, d_ids, d_dists, st))) return r;
-      if ((r = launch_exact_scan(idx, P.small, P.cnt + DP_NSMALL, 0, 148 * 8, d_desc, d_q, k, d_ids, d_dists, st)))
-        return r;
-      FKNN_CUDA(cudaEventRecord(G.ev[3], st));
+      FKNN_CUDA(cudaStreamWaitEvent(st, G.join, 0));
+      FKNN_CUDA(cudaEventRecordWithFlags(G.ev[3], st, cudaEventRecordExternal));  // an event node of the graph
       FKNN_CUDA(cudaGetLastError());
       return FKNN_OK;
     };

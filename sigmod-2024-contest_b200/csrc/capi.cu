@@ -91,6 +91,9 @@ static void free_index(fknn_index *idx) {
   cudaDeviceSynchronize();
   idx->graph.release();
   if (idx->graph.cap) cudaStreamDestroy(idx->graph.cap);
+  if (idx->graph.side) cudaStreamDestroy(idx->graph.side);
+  if (idx->graph.fork) cudaEventDestroy(idx->graph.fork);
+  if (idx->graph.join) cudaEventDestroy(idx->graph.join);
   if (idx->side_stream) cudaStreamDestroy(idx->side_stream);
   if (idx->ev_fork) cudaEventDestroy(idx->ev_fork);
   if (idx->ev_join) cudaEventDestroy(idx->ev_join);
@@ -411,7 +414,7 @@ int fknn_index_get_tuning(const fknn_index *index, int mode, fknn_tuning *t) {
 
 int fknn_search(fknn_index *index, const float *qvecs, const float *metas, uint32_t nq, uint32_t k, int mode,
                 uint32_t *ids, float *dists, void *stream) {
-  fknn_search_opts o;
+  fknn_search_opts o{};
   o.mode = mode;
   o.kprime = 0;
   return fknn_search_ex(index, qvecs, metas, nq, k, &o, ids, dists, stream, nullptr);

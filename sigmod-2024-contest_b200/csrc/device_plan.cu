@@ -210,12 +210,15 @@ __global__ void k_dp_lanes(const uint32_t *__restrict__ seg, uint32_t nq, uint32
 }
 
 __global__ void k_dp_tile_init(Tile *__restrict__ tiles, uint32_t *__restrict__ ts_, uint32_t *__restrict__ te_,
-                               uint32_t ntile_max) {
+                               uint32_t ntile_max, uint32_t *__restrict__ ord_key, uint32_t nitems_max) {
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntile_max; t += gridDim.x * blockDim.x) {
     tiles[t] = Tile{0, 0, 0, 0};
     ts_[t] = 0xffffffffu;
     te_[t] = 0u;
   }
+  // item slots past the item count sort last
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < nitems_max; i += gridDim.x * blockDim.x)
+    ord_key[i] = 0xffffffffu;
 }
 
 // per big query: its tile's first position, count, row range and order;
@@ -293,7 +296,7 @@ __global__ void k_dp_items(const uint32_t *__restrict__ tS, const uint32_t *__re
                            const uint32_t *__restrict__ chunk, const uint32_t *__restrict__ nit_incl,
                            uint32_t blk_rows, uint32_t tq, uint32_t ntile_max, uint32_t nitems_max,
                            uint32_t *__restrict__ cnt, Tile *__restrict__ tiles, WorkItem *__restrict__ items,
-                           int *__restrict__ err) {
+                           uint32_t *__restrict__ ord_key, uint32_t *__restrict__ ord_val, int *__restrict__ err) {
   const uint32_t ntile = cnt[C_NTILE];
   for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < ntile; t += gridDim.x * blockDim.x) {
     const uint32_t c = chunk[t], b0 = tS[t] / blk_rows, b1 = b0 + nblk[t];
@@ -314,6 +317,9 @@ __global__ void k_dp_items(const uint32_t *__restrict__ tS, const uint32_t *__re
       w.blk1 = min(b1, w.blk0 + c);
       w.pad = 0;
       items[first + j] = w;
+      // longest first after the sort (ties keep the item order: the sort is stable)
+      ord_key[first + j] = 0xfffffffeu - (w.blk1 - w.blk0);
+      ord_val[first + j] = first + j;
       add_u64(cnt + C_PAIRS_SCR, (uint64_t)(w.blk1 - w.blk0) * blk_rows * tq);
     }
     if (t == ntile - 1) cnt[C_NITEMS] = min(nit_incl[t], nitems_max);
@@ -339,7 +345,8 @@ DevPlanSizes device_plan_sizes(const fknn_index *idx, uint32_t nq, const PlanSha
 size_t device_plan_bytes(uint32_t nq, const DevPlanSizes &z) {
   const size_t q = (size_t)nq + 1, t = (size_t)z.ntile_max + 1;
   const size_t nb = ((size_t)nq + SC_TILE - 1) / SC_TILE + ((size_t)z.ntile_max + SC_TILE - 1) / SC_TILE + 2;
-  return 256 * 24 + 4 * (12 * q + 7 * t + nb) + sizeof(Tile) * t + sizeof(WorkItem) * (z.nitems_max + 1) + 64 * 4;
+  const size_t it = (size_t)z.nitems_max + 1;
+  return 256 * 28 + 4 * (12 * q + 6 * t + 4 * it + nb) + sizeof(Tile) * t + sizeof(WorkItem) * it + 64 * 4 + 64;
 }
 
 // Lays a DevPlan out in one device buffer of device_plan_bytes bytes.
@@ -373,7 +380,12 @@ void device_plan_layout(DevPlan &P, void *mem, uint32_t nq, const DevPlanSizes &
   P.nblk = (uint32_t *)take(t * 4);
   P.chunk = (uint32_t *)take(t * 4);
   P.nit = (uint32_t *)take(t * 4);
-  P.spare = (uint32_t *)take(t * 4);
+  const size_t it = (size_t)z.nitems_max + 1;
+  P.ord_key = (uint32_t *)take(it * 4);
+  P.ord_val = (uint32_t *)take(it * 4);
+  P.ord_k2 = (uint32_t *)take(it * 4);
+  P.ord_v2 = (uint32_t *)take(it * 4);
+  P.queue = (uint32_t *)take(64);
   P.bsum = (uint32_t *)take((((size_t)nq + SC_TILE - 1) / SC_TILE + ((size_t)z.ntile_max + SC_TILE - 1) / SC_TILE + 2) * 4);
   P.tiles = (Tile *)take(sizeof(Tile) * t);
   P.items = (WorkItem *)take(sizeof(WorkItem) * (z.nitems_max + 1));
@@ -399,7 +411,9 @@ int device_plan_build(fknn_index *idx, const QueryDesc *d_desc, const float *d_m
   scan_incl<OpMax>(P.seg, nq, P.bsum, st);
   k_dp_lanes<<<grid_for(nq), DP_THREADS, 0, st>>>(P.seg, nq, (uint32_t)shape.tq, P.cnt, P.lane, P.tflag);
   scan_incl<OpSum>(P.tflag, nq, P.bsum, st);
-  k_dp_tile_init<<<grid_for(z.ntile_max), DP_THREADS, 0, st>>>(P.tiles, P.tS, P.tE, z.ntile_max);
+  k_dp_tile_init<<<grid_for(std::max(z.ntile_max, z.nitems_max)), DP_THREADS, 0, st>>>(P.tiles, P.tS, P.tE,
+                                                                                      z.ntile_max, P.ord_key,
+                                                                                      z.nitems_max);
   k_dp_tiles<<<grid_for(nq), DP_THREADS, 0, st>>>(P.vals, P.key_hi, d_desc, P.tflag, P.lane, nq, z.ntile_max, P.cnt,
                                                   P.tile_first, P.tiles, P.tS, P.tE, P.big_q, P.big_tile, P.big_lane,
                                                   idx->d_flag);
@@ -411,8 +425,11 @@ int device_plan_build(fknn_index *idx, const QueryDesc *d_desc, const float *d_m
   scan_incl<OpSum>(P.nit, z.ntile_max, P.bsum, st);
   k_dp_items<<<grid_for(z.ntile_max), DP_THREADS, 0, st>>>(P.tS, P.nblk, P.chunk, P.nit, (uint32_t)shape.blk_rows,
                                                            (uint32_t)shape.tq, z.ntile_max, z.nitems_max, P.cnt,
-                                                           P.tiles, P.items, idx->d_flag);
+                                                           P.tiles, P.items, P.ord_key, P.ord_val, idx->d_flag);
   g_launches += 9;
+  // processing order of the work items (longest first) and the queues
+  if ((rc = radix_sort_pairs(idx, P.ord_key, P.ord_val, P.ord_k2, P.ord_v2, z.nitems_max, 0, 32, st))) return rc;
+  FKNN_CUDA(cudaMemsetAsync(P.queue, 0, 64, st));
   FKNN_CUDA(cudaGetLastError());
   return FKNN_OK;
 }

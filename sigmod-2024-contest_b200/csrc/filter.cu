@@ -3,23 +3,30 @@
 // int32(v), 2 l <= ts <= r, 3 both) applied to whole columns, writing each
 // predicate's passing row ids in increasing order.
 //
-// One pass over the columns for up to FP_MAXP predicates (k_filter_scan,
-// a single-pass scan):
-//   * a CTA takes the next 4,096-row tile from a ticket counter, so every
-//     tile before it is already running or done;
-//   * its threads load the tile's labels and timestamps as float4 (16 rows
-//     each, coalesced) and evaluate every predicate on them;
-//   * per predicate the tile publishes its passing count at once, then sums
-//     the counts of all the tiles before it (each thread a strided share, so
-//     no tile waits on another tile's prefix: only on counts published
-//     right after their loads), and every passing row writes its id at
-//     prefix + its rank in the tile.
-// A status word holds its flag and its value together, so one 64-bit
-// volatile load sees a consistent pair.  The waits are bounded by the
-// global timer; a tile that gives up makes that predicate's count
-// UINT64_MAX.  Nothing is read back: the counts land in device memory, so
-// a batch of calls streams back to back.  Algorithmic traffic per launch:
-// 8 B per row plus 4 B per passing row.
+// One cooperative launch per group of up to FP_MAXP predicates reads the
+// columns once (k_filter_coop).  Every CTA owns a contiguous run of rows
+// per round:
+//   1. it streams its labels and timestamps (float4 loads, a few steps in
+//      flight per warp), evaluates every predicate and keeps, per 128-row
+//      warp segment and predicate, four ballot words of pass bits and their
+//      count in shared memory;
+//   2. it scans the segment counts into offsets inside the CTA and
+//      publishes its per-predicate totals;
+//   3. one grid barrier (all CTAs are resident: cooperative launch), after
+//      which each CTA sums the totals of the CTAs before it;
+//   4. it writes the ids of its passing rows from the bits, at CTA offset +
+//      segment offset + rank in the segment.
+// The columns are never re-read, so the traffic is the algorithmic one:
+// 8 B per row plus 4 B per passing row.  A round covers as many rows as the
+// bits of all CTAs hold (one round up to ~12M rows at 16 predicates).
+//
+// The grid barrier is a 64-bit arrival counter that is never reset: the
+// host keeps its value at each launch, and the counter sits in a buffer
+// cleared once.  Its wait is bounded by the global timer; a CTA that gives
+// up marks the launch failed (a flag word tagged with the launch's epoch)
+// and writes UINT64_MAX counts, and CTA 0 writes the real counts only
+// when no CTA failed.  Nothing is read back: the counts land in device
+// memory, so a batch of calls streams back to back, one launch each.
 #include <algorithm>
 #include <cstring>
 
@@ -29,184 +36,228 @@ namespace fknn {
 
 namespace {
 
-constexpr int FS_THREADS = 256;
-constexpr int FS_NW = FS_THREADS / 32;
-constexpr int FS_IT = 4;                          // float4 loads per column per thread
-constexpr int FS_TILE = FS_THREADS * 4 * FS_IT;   // 4,096 rows per tile
-constexpr int FS_SEG = FS_IT * FS_NW;             // 128-row warp segments per tile (= 32)
-constexpr uint32_t FP_MAXP = 16;                  // predicates per launch
-constexpr uint64_t ST_AGG = 1ull << 62, ST_FLAGS = 3ull << 62;
-constexpr uint32_t FS_UNROLL = 4;                 // status words in flight per thread
+constexpr int FC_THREADS = 512;
+constexpr int FC_WARPS = FC_THREADS / 32;
+constexpr int FC_STEP = FC_THREADS * 4;  // rows per CTA step: a float4 of each column per thread
+constexpr int FC_SEG = 128;              // rows per warp segment
+constexpr int FC_DEPTH = 4;              // steps in flight per warp
+constexpr uint32_t FP_MAXP = 16;         // predicates per launch
+constexpr size_t FC_SMEM_MAX = 100 * 1024;  // bits + offsets per CTA, so that two CTAs share an SM
 
-static_assert(FS_SEG == 32, "one warp scans the tile's segments");
+static_assert(FC_WARPS >= (int)FP_MAXP, "one warp per predicate sums the CTA totals");
 
 struct FilterPreds {
   float4 m[FP_MAXP];  // (type, v, l, r), checked on the host
 };
 
-__device__ __forceinline__ bool pred_pass(const float4 &m, int32_t lab, float t) {
+// 4 pass bits (rows 4 * lane + c) of one predicate
+__device__ __forceinline__ uint32_t pred_bits4(const float4 &m, const float4 &lab, const float4 &t) {
   const uint32_t type = (uint32_t)m.x;
   const int32_t v = (int32_t)m.y;
-  switch (type) {
-    case 0: return true;
-    case 1: return lab == v;
-    case 2: return t >= m.z && t <= m.w;
-    default: return lab == v && t >= m.z && t <= m.w;
-  }
+  const bool c0 = type == 0 || type == 2, t0 = type == 0 || type == 1;  // label test skipped / time test skipped
+  auto one = [&](float l, float ts) -> uint32_t {
+    const bool cat = c0 || (int32_t)l == v;
+    const bool tim = t0 || (ts >= m.z && ts <= m.w);
+    return (cat && tim) ? 1u : 0u;
+  };
+  return one(lab.x, t.x) | (one(lab.y, t.y) << 1) | (one(lab.z, t.z) << 2) | (one(lab.w, t.w) << 3);
 }
 
 __device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t *p) { return *(const volatile uint64_t *)p; }
 
-// status: np x ntiles words and the ticket after them, zeroed before the
-// launch.  Grid: ntiles CTAs.
-__global__ void __launch_bounds__(FS_THREADS) k_filter_scan(const float *__restrict__ labels,
-                                                            const float *__restrict__ ts, uint64_t n,
-                                                            FilterPreds P, uint32_t np, uint32_t ntiles,
-                                                            uint64_t *__restrict__ status, uint32_t *ticket,
-                                                            uint32_t *__restrict__ out, uint64_t out_stride,
-                                                            uint64_t *__restrict__ counts) {
+// Loads one step's float4 of each column for this thread (rows r .. r + 3;
+// past n: zeros and valid bits cleared).
+__device__ __forceinline__ void load_step(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n,
+                                          uint64_t r, float4 &a, float4 &b, uint32_t &valid) {
+  if (r + 4 <= n) {
+    a = __ldcs(reinterpret_cast<const float4 *>(labels + r));
+    b = __ldcs(reinterpret_cast<const float4 *>(ts + r));
+    valid = 0xfu;
+  } else {
+    float la[4] = {0.f, 0.f, 0.f, 0.f}, tb[4] = {0.f, 0.f, 0.f, 0.f};
+    valid = 0;
+    for (int c = 0; c < 4; ++c)
+      if (r + c < n) {
+        la[c] = labels[r + c];
+        tb[c] = ts[r + c];
+        valid |= 1u << c;
+      }
+    a = make_float4(la[0], la[1], la[2], la[3]);
+    b = make_float4(tb[0], tb[1], tb[2], tb[3]);
+  }
+}
+
+// Grid: G CTAs, all resident.  Rows per CTA per round: R (a multiple of
+// FC_STEP).  Dynamic shared memory: np x nseg x uint4 bits, then np x nseg
+// offsets (nseg = R / FC_SEG).  sync: [0] the arrival counter (value
+// bar_base at this launch), [1] the failure flag, [2 ..] 2 x G x FP_MAXP
+// per-round CTA totals (double-buffered by round parity).
+__global__ void __launch_bounds__(FC_THREADS, 2)
+    k_filter_coop(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n, FilterPreds P,
+                  uint32_t np, uint32_t R, uint32_t rounds, uint64_t *sync, uint64_t bar_base, uint32_t ep,
+                  uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts) {
+  extern __shared__ __align__(16) unsigned char fc_smem[];
+  const uint32_t nseg = R / FC_SEG;
+  uint4 *bits = reinterpret_cast<uint4 *>(fc_smem);                           // [np][nseg]
+  uint32_t *segoff = reinterpret_cast<uint32_t *>(bits + (size_t)np * nseg);  // [np][nseg]
   __shared__ float4 pm[FP_MAXP];
-  __shared__ uint32_t seg[FS_SEG];
-  __shared__ uint32_t s_tile, s_total;
-  __shared__ uint64_t s_prefix, s_part[FS_NW];
-  __shared__ int s_fail[FS_NW];
+  __shared__ uint32_t wtot[FP_MAXP][FC_WARPS];
+  __shared__ uint64_t s_off[FP_MAXP], s_base[FP_MAXP];
+  __shared__ int s_fail;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
-  if (tid < (int)FP_MAXP) pm[tid] = P.m[tid];
-  if (tid == 0) s_tile = atomicAdd(ticket, 1u);
+  const uint32_t G = gridDim.x, cta = blockIdx.x;
+  const uint32_t nsteps = R / FC_STEP;
+  if (tid < (int)FP_MAXP) {
+    pm[tid] = P.m[tid];
+    s_base[tid] = 0;
+  }
   __syncthreads();
-  const uint32_t t = s_tile;
-  const uint64_t base = (uint64_t)t * FS_TILE;
-  // this thread's rows: base + it*1024 + 4*tid + c, c = 0..3
-  int32_t lab[FS_IT][4];
-  float tv[FS_IT][4];
-  uint32_t valid = 0;  // bit it*4+c: the row is inside the base
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sync);
+  uint64_t *flag = sync + 1, *part = sync + 2;
+  const uint32_t lanemask_lt = (1u << lane) - 1u;
+
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint64_t row0 = ((uint64_t)rd * G + cta) * R;
+    // ---- 1. pass bits and counts per warp segment (segment s * FC_WARPS + w)
+    float4 la[FC_DEPTH], tb[FC_DEPTH];
+    uint32_t vb[FC_DEPTH];
 #pragma unroll
-  for (int it = 0; it < FS_IT; ++it) {
-    const uint64_t r = base + (uint64_t)it * (FS_THREADS * 4) + 4 * tid;
-    if (r + 4 <= n) {
-      const float4 a = __ldcs(reinterpret_cast<const float4 *>(labels + r));
-      const float4 b = __ldcs(reinterpret_cast<const float4 *>(ts + r));
-      lab[it][0] = (int32_t)a.x;
-      lab[it][1] = (int32_t)a.y;
-      lab[it][2] = (int32_t)a.z;
-      lab[it][3] = (int32_t)a.w;
-      tv[it][0] = b.x;
-      tv[it][1] = b.y;
-      tv[it][2] = b.z;
-      tv[it][3] = b.w;
-      valid |= 0xfu << (it * 4);
-    } else {
+    for (int d = 0; d < FC_DEPTH; ++d)
+      if ((uint32_t)d < nsteps)
+        load_step(labels, ts, n, row0 + (uint64_t)d * FC_STEP + w * FC_SEG + 4 * lane, la[d], tb[d], vb[d]);
+    for (uint32_t s0 = 0; s0 < nsteps; s0 += FC_DEPTH) {
 #pragma unroll
-      for (int c = 0; c < 4; ++c) {
-        lab[it][c] = 0;
-        tv[it][c] = 0.f;
-        if (r + c < n) {
-          lab[it][c] = (int32_t)labels[r + c];
-          tv[it][c] = ts[r + c];
-          valid |= 1u << (it * 4 + c);
+      for (int d = 0; d < FC_DEPTH; ++d) {
+        const uint32_t s = s0 + d;
+        if (s < nsteps) {
+          const uint32_t seg = s * FC_WARPS + w;
+          for (uint32_t p = 0; p < np; ++p) {
+            const uint32_t b4 = pred_bits4(pm[p], la[d], tb[d]) & vb[d];
+            const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
+            const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
+            if (lane == 0) {
+              bits[(size_t)p * nseg + seg] = make_uint4(m0, m1, m2, m3);
+              segoff[(size_t)p * nseg + seg] = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+            }
+          }
+          const uint32_t sn = s + FC_DEPTH;  // the step this slot carries next
+          if (sn < nsteps)
+            load_step(labels, ts, n, row0 + (uint64_t)sn * FC_STEP + w * FC_SEG + 4 * lane, la[d], tb[d], vb[d]);
         }
       }
-    }
-  }
-  for (uint32_t p = 0; p < np; ++p) {
-    const float4 m = pm[p];
-    uint32_t mask = 0;
-#pragma unroll
-    for (int it = 0; it < FS_IT; ++it)
-#pragma unroll
-      for (int c = 0; c < 4; ++c) mask |= (pred_pass(m, lab[it][c], tv[it][c]) ? 1u : 0u) << (it * 4 + c);
-    mask &= valid;
-    // rank of this lane's rows inside its warp's 128-row segment of each it
-    uint32_t excl[FS_IT];
-#pragma unroll
-    for (int it = 0; it < FS_IT; ++it) {
-      const uint32_t cnt = __popc((mask >> (it * 4)) & 0xfu);
-      uint32_t inc = cnt;
-#pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += v;
-      }
-      excl[it] = inc - cnt;
-      if (lane == 31) seg[it * FS_NW + w] = inc;
     }
     __syncthreads();
-    uint64_t *st = status + (uint64_t)p * ntiles;
-    if (w == 0) {
-      // the 32 segments in row order (it-major, then warp): exclusive offsets
-      const uint32_t v = seg[lane];
-      uint32_t inc = v;
+    // ---- 2. segment offsets inside the CTA (segments in row order), totals
+    for (uint32_t i0 = 0; i0 < nseg; i0 += FC_THREADS) {
+      const uint32_t i = i0 + tid;
+      for (uint32_t p = 0; p < np; ++p) {
+        const uint32_t v = i < nseg ? segoff[(size_t)p * nseg + i] : 0u;
+        uint32_t inc = v;
 #pragma unroll
-      for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
-        if (lane >= o) inc += x;
-      }
-      seg[lane] = inc - v;
-      if (lane == 31) {
-        s_total = inc;
-        *(volatile uint64_t *)(st + t) = ST_AGG | inc;  // published before this tile waits on anything
-      }
-    }
-    // the tile's prefix: every thread sums a strided share of the counts the
-    // tiles before it published (they took their tickets first, so they run
-    // and publish without waiting); the waits are bounded
-    uint64_t part = 0;
-    bool failed = false;
-    const uint64_t t0 = global_ns();
-    for (uint32_t j0 = tid; j0 < t && !failed; j0 += FS_UNROLL * FS_THREADS) {
-      uint64_t sv[FS_UNROLL];
-#pragma unroll
-      for (uint32_t u = 0; u < FS_UNROLL; ++u) {
-        const uint32_t j = j0 + u * FS_THREADS;
-        sv[u] = j < t ? ld_volatile_u64(st + j) : ST_AGG;  // independent loads, in flight together
-      }
-#pragma unroll
-      for (uint32_t u = 0; u < FS_UNROLL; ++u) {
-        while (!failed && (sv[u] & ST_FLAGS) == 0) {
-          if (global_ns() - t0 > WAIT_NS) failed = true;
-          else sv[u] = ld_volatile_u64(st + j0 + u * FS_THREADS);
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += x;
         }
-        part += sv[u] & 0xffffffffull;
+        if (i < nseg) segoff[(size_t)p * nseg + i] = inc - v;  // exclusive within the warp's 32 segments
+        if (lane == 31) wtot[p][w] = inc;
       }
+      __syncthreads();
+      if (tid < (int)np) {  // the warps' totals -> exclusive prefixes, carried across chunks of segments
+        uint32_t acc = 0;
+        for (int j = 0; j < FC_WARPS; ++j) {
+          const uint32_t x = wtot[tid][j];
+          wtot[tid][j] = acc;
+          acc += x;
+        }
+        // s_off holds the running total of the earlier chunks
+        const uint64_t carry = i0 ? s_off[tid] : 0u;
+        for (int j = 0; j < FC_WARPS; ++j) wtot[tid][j] += (uint32_t)carry;
+        s_off[tid] = carry + acc;
+      }
+      __syncthreads();
+      if (i < nseg)
+        for (uint32_t p = 0; p < np; ++p) segoff[(size_t)p * nseg + i] += wtot[p][w];
+      __syncthreads();
     }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
-    const uint32_t anyfail = __ballot_sync(0xffffffffu, failed);
-    if (lane == 0) {
-      s_part[w] = part;
-      s_fail[w] = anyfail ? 1 : 0;
+    // the CTA's totals for this round
+    uint64_t *mypart = part + ((size_t)(rd & 1) * G + cta) * FP_MAXP;
+    if (tid < (int)np) {
+      mypart[tid] = s_off[tid];
+      __threadfence();  // visible to every CTA before this CTA arrives at the barrier
     }
+    // ---- 3. grid barrier (bounded)
     __syncthreads();
     if (tid == 0) {
-      uint64_t pre = 0;
+      __threadfence();
+      atomicAdd(bar, 1ull);
+      const uint64_t target = bar_base + (uint64_t)(rd + 1) * G;
       int f = 0;
-#pragma unroll
-      for (int j = 0; j < FS_NW; ++j) {
-        pre += s_part[j];
-        f |= s_fail[j];
+      if (ld_volatile_u64(sync) < target) {
+        const uint64_t t0 = global_ns();
+        while (ld_volatile_u64(sync) < target) {
+          if (global_ns() - t0 > WAIT_NS) {
+            f = 1;
+            break;
+          }
+          __nanosleep(64);
+        }
       }
-      s_prefix = f ? ~0ull : pre;
-      // the count: the last tile's prefix plus its own; a tile that gave up
-      // raises it to UINT64_MAX (counts start at 0, combined by max)
-      unsigned long long *cp = reinterpret_cast<unsigned long long *>(counts + p);
-      if (f) atomicMax(cp, ~0ull);
-      else if (t == ntiles - 1) atomicMax(cp, (unsigned long long)(pre + s_total));
+      __threadfence();
+      s_fail = f;
     }
     __syncthreads();
-    const uint64_t prefix = s_prefix;
-    if (prefix != ~0ull) {
-      uint32_t *op = out + (uint64_t)p * out_stride;
+    if (s_fail) {
+      // this launch's outputs are incomplete: flag it, poison the counts
+      if (tid == 0) {
+        *(volatile uint64_t *)flag = ep;
+        __threadfence();
+      }
+      __syncthreads();
+      if (tid < (int)np) counts[tid] = ~0ull;
+      return;
+    }
+    // ---- the CTAs before this one: this CTA's offset; all: the round total
+    if (w < (int)np) {
+      const uint64_t *rp = part + (size_t)(rd & 1) * G * FP_MAXP;
+      uint64_t before = 0, all = 0;
+      for (uint32_t c = lane; c < G; c += 32) {
+        const uint64_t x = __ldcg(rp + (size_t)c * FP_MAXP + w);
+        all += x;
+        if (c < cta) before += x;
+      }
 #pragma unroll
-      for (int it = 0; it < FS_IT; ++it) {
-        const uint32_t mk = (mask >> (it * 4)) & 0xfu;
-        uint32_t pos = (uint32_t)prefix + seg[it * FS_NW + w] + excl[it];
-        const uint64_t r = base + (uint64_t)it * (FS_THREADS * 4) + 4 * tid;
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if ((mk >> c) & 1u) op[pos++] = (uint32_t)(r + c);
+      for (int o = 16; o > 0; o >>= 1) {
+        before += __shfl_xor_sync(0xffffffffu, before, o);
+        all += __shfl_xor_sync(0xffffffffu, all, o);
+      }
+      if (lane == 0) {
+        s_off[w] = s_base[w] + before;
+        s_base[w] += all;
       }
     }
-    __syncthreads();  // seg and s_prefix are rewritten for the next predicate
+    __syncthreads();
+    // ---- 4. ids of the passing rows, from the bits
+    for (uint32_t s = 0; s < nsteps; ++s) {
+      const uint32_t seg = s * FC_WARPS + w;
+      const uint64_t r = row0 + (uint64_t)s * FC_STEP + w * FC_SEG + 4 * lane;
+      for (uint32_t p = 0; p < np; ++p) {
+        const uint4 m = bits[(size_t)p * nseg + seg];
+        const uint32_t b4 = ((m.x >> lane) & 1u) | (((m.y >> lane) & 1u) << 1) | (((m.z >> lane) & 1u) << 2) |
+                            (((m.w >> lane) & 1u) << 3);
+        if (!__any_sync(0xffffffffu, b4)) continue;
+        uint32_t pos = (uint32_t)s_off[p] + segoff[(size_t)p * nseg + seg] + __popc(m.x & lanemask_lt) +
+                       __popc(m.y & lanemask_lt) + __popc(m.z & lanemask_lt) + __popc(m.w & lanemask_lt);
+        uint32_t *op = out + (uint64_t)p * out_stride;
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+          if ((b4 >> c) & 1u) op[pos++] = (uint32_t)(r + c);
+      }
+    }
+    __syncthreads();  // bits and offsets are rewritten by the next round
+  }
+  if (cta == 0 && tid < (int)np) {
+    const bool failed = ld_volatile_u64(flag) == ep;
+    counts[tid] = failed ? ~0ull : s_base[tid];
   }
 }
 
@@ -234,25 +285,56 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
                       cudaStream_t st) {
   const uint64_t n = idx->n;
   if (np == 0) return FKNN_OK;
-  const uint32_t ntiles = (uint32_t)((n + FS_TILE - 1) / FS_TILE);
-  const uint32_t pmax = std::min<uint32_t>(np, FP_MAXP);
-  // per launch: status words (predicates x tiles) and the ticket, cleared first
-  uint64_t *status;
+  FilterState &fs = idx->filter_state;
+  // resident CTAs of the cooperative grid (two per SM when the shared memory allows)
+  if (!fs.grid) {
+    FKNN_CUDA(cudaFuncSetAttribute(k_filter_coop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)FC_SMEM_MAX));
+    int per_sm = 0;
+    FKNN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_filter_coop, FC_THREADS, FC_SMEM_MAX));
+    if (per_sm < 1) {
+      set_error("fknn_filter_rows: the compaction kernel does not fit an SM");
+      return FKNN_ECUDA;
+    }
+    fs.grid = (uint32_t)idx->num_sms * (uint32_t)std::min(per_sm, 2);
+  }
+  const uint32_t G = fs.grid;
+  // sync words: arrival counter, failure flag, 2 x G x FP_MAXP CTA totals;
+  // cleared when the buffer is new or the epochs run out
+  const size_t words = 2 + 2 * (size_t)G * FP_MAXP;
+  uint64_t *sync;
   int rc;
-  if ((rc = ws_get(idx, 16, ((size_t)pmax * ntiles + 1) * sizeof(uint64_t), (void **)&status))) return rc;
+  if ((rc = ws_get(idx, 16, words * sizeof(uint64_t), (void **)&sync))) return rc;
+  if (fs.status != sync || fs.bytes != idx->ws[16].bytes || fs.epoch >= (1u << 30)) {
+    FKNN_CUDA(cudaMemsetAsync(sync, 0, words * sizeof(uint64_t), st));
+    fs.status = sync;
+    fs.bytes = idx->ws[16].bytes;
+    fs.epoch = 0;
+    fs.arrivals = 0;
+  }
   for (uint32_t p0 = 0; p0 < np; p0 += FP_MAXP) {
     const uint32_t m = std::min<uint32_t>(FP_MAXP, np - p0);
+    // rows per CTA per round: as few rounds as the bits allow, rows split evenly
+    const size_t per_row = (size_t)m * (sizeof(uint4) + sizeof(uint32_t));  // per 128-row segment
+    const uint64_t r_cap = std::max<uint64_t>(FC_STEP, (FC_SMEM_MAX / per_row) * FC_SEG / FC_STEP * FC_STEP);
+    const uint64_t rounds = std::max<uint64_t>(1, (n + (uint64_t)G * r_cap - 1) / ((uint64_t)G * r_cap));
+    const uint64_t per_cta = (n + (uint64_t)G * rounds - 1) / ((uint64_t)G * rounds);
+    const uint32_t R = (uint32_t)std::max<uint64_t>(FC_STEP, (per_cta + FC_STEP - 1) / FC_STEP * FC_STEP);
+    const size_t smem = (size_t)(R / FC_SEG) * per_row;
     FilterPreds P;
     std::memset(&P, 0, sizeof(P));
     for (uint32_t p = 0; p < m; ++p) {
       const float *q = metas + (size_t)(p0 + p) * 4;
       P.m[p] = make_float4(q[0], q[1], q[2], q[3]);
     }
-    uint32_t *ticket = reinterpret_cast<uint32_t *>(status + (size_t)m * ntiles);
-    FKNN_CUDA(cudaMemsetAsync(status, 0, ((size_t)m * ntiles + 1) * sizeof(uint64_t), st));
-    FKNN_CUDA(cudaMemsetAsync(d_counts + p0, 0, (size_t)m * sizeof(uint64_t), st));
-    k_filter_scan<<<ntiles, FS_THREADS, 0, st>>>(idx->labels_f, idx->ts_f, n, P, m, ntiles, status, ticket,
-                                                 d_out + (uint64_t)p0 * n, n, d_counts + p0);
+    const float *lab = idx->labels_f, *tsv = idx->ts_f;
+    uint64_t nn = n, bar_base = fs.arrivals, stride = n;
+    uint32_t mm = m, RR = R, nr = (uint32_t)rounds, ep = ++fs.epoch;
+    uint32_t *o = d_out + (uint64_t)p0 * n;
+    uint64_t *c = d_counts + p0;
+    void *args[] = {(void *)&lab, (void *)&tsv, (void *)&nn, (void *)&P, (void *)&mm, (void *)&RR, (void *)&nr,
+                    (void *)&sync, (void *)&bar_base, (void *)&ep, (void *)&o, (void *)&stride, (void *)&c};
+    FKNN_CUDA(cudaLaunchCooperativeKernel((const void *)k_filter_coop, dim3(G), dim3(FC_THREADS), args, smem, st));
+    fs.arrivals += rounds * G;
     g_launches += 1;
   }
   FKNN_CUDA(cudaGetLastError());

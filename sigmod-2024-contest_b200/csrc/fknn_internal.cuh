@@ -184,7 +184,10 @@ struct DevPlan {
   uint32_t *seg = nullptr, *lane = nullptr, *tflag = nullptr;
   uint32_t *big_q = nullptr, *big_tile = nullptr, *big_lane = nullptr, *small = nullptr;
   uint32_t *tile_first = nullptr, *tS = nullptr, *tE = nullptr, *nblk = nullptr, *chunk = nullptr, *nit = nullptr;
-  uint32_t *spare = nullptr, *bsum = nullptr;
+  uint32_t *bsum = nullptr;
+  // the work items longest first (ord_val after the sort), for a work queue
+  uint32_t *ord_key = nullptr, *ord_val = nullptr, *ord_k2 = nullptr, *ord_v2 = nullptr;
+  uint32_t *queue = nullptr;  // two work-queue counters (pilot pass, main pass), cleared by the plan
   Tile *tiles = nullptr;
   WorkItem *items = nullptr;
 };
@@ -206,6 +209,8 @@ struct GraphCache {
   uint32_t launches = 0;   // kernels in the graph
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};  // screen / merge / scan boundaries
   cudaStream_t cap = nullptr;  // the capture runs here: the caller's stream may be the legacy one
+  cudaStream_t side = nullptr;  // a second branch of the graph (the short-slab scans)
+  cudaEvent_t fork = nullptr, join = nullptr;
   void release() {
     if (exec) cudaGraphExecDestroy(exec);
     exec = nullptr;
@@ -214,6 +219,18 @@ struct GraphCache {
       if (e) cudaEventDestroy(e);
     for (auto &e : ev) e = nullptr;
   }
+};
+
+// The predicate compaction's persistent state over its sync buffer (ws
+// slot 16): the grid barrier counts arrivals on a counter that is never
+// reset, and launches tag their failure flag with an epoch, so no launch
+// clears anything.
+struct FilterState {
+  const void *status = nullptr;  // the buffer the state belongs to ...
+  size_t bytes = 0;              // ... and its size (a regrown buffer may reuse the address)
+  uint32_t epoch = 0;            // the last launch's epoch
+  uint64_t arrivals = 0;         // barrier arrivals so far (the counter's value)
+  uint32_t grid = 0;             // resident CTAs of the cooperative launch (0: not yet measured)
 };
 
 // Grow-only device arena for per-call scratch.
@@ -265,6 +282,7 @@ struct fknn_index {
   bool test_withhold = false;
   // captured searches (fknn_search_opts.flags & FKNN_SEARCH_CAPTURE)
   fknn::GraphCache graph;
+  fknn::FilterState filter_state;
 };
 
 namespace fknn {

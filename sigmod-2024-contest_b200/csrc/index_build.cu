@@ -299,6 +299,7 @@ int build_index_from_columns(fknn_index *idx, cudaStream_t st) {
   FKNN_CUDA(cudaGetLastError());
   uint32_t runs = 0;
   FKNN_CUDA(cudaMemcpyAsync(&runs, idx->d_flag, 4, cudaMemcpyDeviceToHost, st));
+  FKNN_CUDA(cudaMemsetAsync(idx->d_flag, 0, sizeof(int), st));
   FKNN_CUDA(cudaStreamSynchronize(st));
   idx->n_labels = runs ? runs : 1;
   return FKNN_OK;

@@ -416,6 +416,13 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
   }
   if (nq == 0) return FKNN_OK;
   const auto t0 = std::chrono::steady_clock::now();
+  auto tl = t0;
+  auto lap = [&tl]() {  // ms since the last lap (stage boundaries are host syncs)
+    const auto t = std::chrono::steady_clock::now();
+    const float ms = std::chrono::duration<float, std::milli>(t - tl).count();
+    tl = t;
+    return ms;
+  };
   fknn_router_stats S{};
   FKNN_CUDA(cudaSetDevice(r->device));
   cudaStream_t st = r->st;
@@ -466,6 +473,7 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
     }
   }
   S.n_bruteforce = (uint32_t)bf.size();
+  S.ms_prepare = lap();
   S.n_type0 = (uint32_t)type0.size();
   S.n_type2 = (uint32_t)type2.size();
 
@@ -521,6 +529,7 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
     g_launches += 2;
     if ((rc = rerank_rows(bf, kb))) return rc;
   }
+  S.ms_bruteforce = lap();
 
   // 2. category graphs (hybrid_graph.cpp:239-298): pool ceil(ef_min +
   //    slope * category size), graph_refine_k candidates, FP32 re-rank
@@ -560,6 +569,8 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
     }
   }
 
+  S.ms_category = lap();
+
   // 3. types 0 and 2: candidates of several time buckets merged per query
   //    into a pool of graph_refine_k (maxPQIFCS<int>), then FP32 re-rank
   std::vector<fknn::IntPool> pool(nq);
@@ -593,6 +604,7 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
   // type 0: SearchFilterSubTime with ef0_full on every bucket (:303-333)
   for (const fknn_router::Sub &b : r->bks)
     if ((rc = bucket_search(b, FKNN_GRAPH_FILTER_SUBTIME, type0, P.ef0_full, nullptr, nullptr))) return rc;
+  S.ms_type0 = lap();
 
   // type 2: SplitInterval (:91-134) with bf_thr 0.5 when sel < 0.2, else 0.2
   if (!type2.empty()) {
@@ -689,6 +701,7 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
       }
     }
   }
+  S.ms_type2 = lap();
   // global re-rank of the pools (:465-494), ids through the timestamp order
   {
     std::vector<uint32_t> list;
@@ -714,6 +727,7 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
     set_error("fknn_router_search: a candidate named a row outside the base");
     return FKNN_EINVAL;
   }
+  S.ms_final = lap();
   S.ms_total = std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
   if (stats) *stats = S;
   return FKNN_OK;

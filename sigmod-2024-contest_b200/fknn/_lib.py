@@ -140,7 +140,9 @@ class RouterParams(Structure):
 
 class RouterStats(Structure):
     _fields_ = [(f, c_uint32) for f in ("n_bruteforce", "n_category", "n_type0", "n_type2", "n_graph_calls",
-                                        "n_split_small", "n_split_medium", "n_split_full")] + [("ms_total", c_float)]
+                                        "n_split_small", "n_split_medium", "n_split_full")] + \
+        [(f, c_float) for f in ("ms_total", "ms_prepare", "ms_bruteforce", "ms_category", "ms_type0", "ms_type2",
+                                "ms_final")]
 
     def as_dict(self) -> dict:
         return {f: getattr(self, f) for f, _ in self._fields_}
