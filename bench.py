@@ -85,6 +85,8 @@ def parse():
     ap.add_argument("--graph", action="store_true",
                     help="graph-path run instead of the headline: per-category HNSW graphs (reference build), "
                          "batched beam search + FP32 re-rank, recall against the exact path; one JSON line per beam")
+    ap.add_argument("--plan", choices=["graph", "host"], default="graph",
+                    help="BF16 leg: plan on the device and replay a captured CUDA graph, or plan on the host")
     ap.add_argument("--router", action="store_true",
                     help="reference-routing run instead of the headline: fknn_router beside the reference pipeline's "
                          "BatchSearch over the same subgraphs; q/s and recall per query type")
@@ -811,12 +813,14 @@ def main():
     def max_over_ranks(x):
         return replicas.max_over_ranks(x, "cuda")
 
-    def timed(mode, kprime, out_ids, steps, warmup):
+    def timed(mode, kprime, out_ids, steps, warmup, graph=False):
         """warmup untimed steps, then `steps` steps between barriers, CUDA
-        events on the launching stream; returns (ms per step, per-step stats)."""
+        events on the launching stream; returns (ms per step, per-step stats).
+        graph: the search planned on the device and replayed as a captured
+        CUDA graph (FKNN_SEARCH_GRAPH)."""
         def step():
             return idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=out_ids, dists=dd,
-                              stream=stream.cuda_stream, return_stats=True)[2]
+                              stream=stream.cuda_stream, return_stats=True, graph=graph)[2]
         for _ in range(warmup):
             step()
         barrier()
@@ -844,7 +848,11 @@ def main():
     exact_ids = ids.cpu().numpy().view(np.uint32).copy()
     exact_d = dd.cpu().numpy().copy()
     ids_b = torch.empty_like(ids)
-    ms_bf16, st_bf16 = timed(fknn.MODE_BF16_RERANK, args.kprime, ids_b, args.steps, args.warmup)
+    use_graph = args.plan == "graph"
+    ms_bf16, st_bf16 = timed(fknn.MODE_BF16_RERANK, args.kprime, ids_b, args.steps, args.warmup, graph=use_graph)
+    # the other planning form of the same search, for comparison (a few steps)
+    ms_bf16_other, _ = timed(fknn.MODE_BF16_RERANK, args.kprime, torch.empty_like(ids), min(args.steps, 5), 1,
+                             graph=not use_graph)
     clk = clocks.stop()
     bf16_ids = ids_b.cpu().numpy().view(np.uint32)
     recall_bf16 = datagen.recall_matrix(bf16_ids, exact_ids)
@@ -883,14 +891,14 @@ def main():
     hids = torch.empty((nq, 100), dtype=torch.int32, pin_memory=True).numpy().view(np.uint32)
     for _ in range(2):
         idx.search(hq, hm, k=100, mode=head_mode, kprime=args.kprime, ids=hids, with_dists=False,
-                   stream=stream.cuda_stream)
+                   stream=stream.cuda_stream, graph=use_graph and use_bf16)
     barrier()
     lat = []
     for _ in range(args.steps):
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record(stream)
         idx.search(hq, hm, k=100, mode=head_mode, kprime=args.kprime, ids=hids, with_dists=False,
-                   stream=stream.cuda_stream)
+                   stream=stream.cuda_stream, graph=use_graph and use_bf16)
         e.record(stream)
         e.synchronize()
         lat.append(s.elapsed_time(e))
@@ -955,7 +963,10 @@ def main():
             "bf16_rerank": {"value": world * nq / (ms_bf16 * 1e-3), "ms_per_step": ms_bf16, "kprime": args.kprime,
                             "recall_at_100_vs_exact_all_queries": recall_bf16,
                             "speedup_vs_exact": ms_exact / ms_bf16,
-                            "n_boundary_f64_per_step": st_bf16[-1]["n_boundary_f64"]},
+                            "n_boundary_f64_per_step": st_bf16[-1]["n_boundary_f64"],
+                            "plan": ("on the device, the whole search one captured CUDA graph" if use_graph
+                                     else "on the host"),
+                            "ms_per_step_other_plan": ms_bf16_other},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(nq * 100 * 4 + nq * 16),
                     "d2h_bytes_per_step": int(nq * 100 * 4), "same_ids_as_device_path": same,
                     "result": "ids (nq x 100 u32), as BatchSearch returns them"},

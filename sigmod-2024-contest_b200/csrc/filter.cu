@@ -28,6 +28,7 @@
 // when no CTA failed.  Nothing is read back: the counts land in device
 // memory, so a batch of calls streams back to back, one launch each.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 
 #include "device_util.cuh"
@@ -43,22 +44,22 @@ constexpr int FC_SEG = 128;              // rows per warp segment
 constexpr int FC_DEPTH = 4;              // steps in flight per warp
 constexpr uint32_t FP_MAXP = 16;         // predicates per launch
 constexpr size_t FC_SMEM_MAX = 100 * 1024;  // bits + offsets per CTA, so that two CTAs share an SM
+constexpr int FC_SUM_UNROLL = 10;           // CTA totals in flight per lane (one pass for up to 320 CTAs)
 
 static_assert(FC_WARPS >= (int)FP_MAXP, "one warp per predicate sums the CTA totals");
 
+// Per predicate the closed intervals a row must fall in:
+// (label lo, label hi, ts lo, ts hi).  The host turns int32(label) == v into
+// the float interval of labels that truncate to v, and open predicates into
+// (-inf, inf), so the device test is four float compares per row.
 struct FilterPreds {
-  float4 m[FP_MAXP];  // (type, v, l, r), checked on the host
+  float4 b[FP_MAXP];
 };
 
 // 4 pass bits (rows 4 * lane + c) of one predicate
-__device__ __forceinline__ uint32_t pred_bits4(const float4 &m, const float4 &lab, const float4 &t) {
-  const uint32_t type = (uint32_t)m.x;
-  const int32_t v = (int32_t)m.y;
-  const bool c0 = type == 0 || type == 2, t0 = type == 0 || type == 1;  // label test skipped / time test skipped
+__device__ __forceinline__ uint32_t pred_bits4(const float4 &b, const float4 &lab, const float4 &t) {
   auto one = [&](float l, float ts) -> uint32_t {
-    const bool cat = c0 || (int32_t)l == v;
-    const bool tim = t0 || (ts >= m.z && ts <= m.w);
-    return (cat && tim) ? 1u : 0u;
+    return (l >= b.x && l <= b.y && ts >= b.z && ts <= b.w) ? 1u : 0u;
   };
   return one(lab.x, t.x) | (one(lab.y, t.y) << 1) | (one(lab.z, t.z) << 2) | (one(lab.w, t.w) << 3);
 }
@@ -67,8 +68,8 @@ __device__ __forceinline__ uint64_t ld_volatile_u64(const uint64_t *p) { return 
 
 // Loads one step's float4 of each column for this thread (rows r .. r + 3;
 // past n: zeros and valid bits cleared).
-__device__ __forceinline__ void load_step(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n,
-                                          uint64_t r, float4 &a, float4 &b, uint32_t &valid) {
+__device__ __forceinline__ void load_step(const float *__restrict__ labels, const float *__restrict__ ts, uint32_t n,
+                                          uint32_t r, float4 &a, float4 &b, uint32_t &valid) {
   if (r + 4 <= n) {
     a = __ldcs(reinterpret_cast<const float4 *>(labels + r));
     b = __ldcs(reinterpret_cast<const float4 *>(ts + r));
@@ -91,16 +92,17 @@ __device__ __forceinline__ void load_step(const float *__restrict__ labels, cons
 // FC_STEP).  Dynamic shared memory: np x nseg x uint4 bits, then np x nseg
 // offsets (nseg = R / FC_SEG).  sync: [0] the arrival counter (value
 // bar_base at this launch), [1] the failure flag, [2 ..] 2 x G x FP_MAXP
-// per-round CTA totals (double-buffered by round parity).
+// per-round CTA totals (double-buffered by round parity).  Row ids fit
+// 32 bits (n < 2^31).
 __global__ void __launch_bounds__(FC_THREADS, 2)
-    k_filter_coop(const float *__restrict__ labels, const float *__restrict__ ts, uint64_t n, FilterPreds P,
+    k_filter_coop(const float *__restrict__ labels, const float *__restrict__ ts, uint32_t n, FilterPreds P,
                   uint32_t np, uint32_t R, uint32_t rounds, uint64_t *sync, uint64_t bar_base, uint32_t ep,
                   uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts) {
   extern __shared__ __align__(16) unsigned char fc_smem[];
   const uint32_t nseg = R / FC_SEG;
   uint4 *bits = reinterpret_cast<uint4 *>(fc_smem);                           // [np][nseg]
   uint32_t *segoff = reinterpret_cast<uint32_t *>(bits + (size_t)np * nseg);  // [np][nseg]
-  __shared__ float4 pm[FP_MAXP];
+  __shared__ float4 pb[FP_MAXP];
   __shared__ uint32_t wtot[FP_MAXP][FC_WARPS];
   __shared__ uint64_t s_off[FP_MAXP], s_base[FP_MAXP];
   __shared__ int s_fail;
@@ -108,7 +110,7 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
   const uint32_t G = gridDim.x, cta = blockIdx.x;
   const uint32_t nsteps = R / FC_STEP;
   if (tid < (int)FP_MAXP) {
-    pm[tid] = P.m[tid];
+    pb[tid] = P.b[tid];
     s_base[tid] = 0;
   }
   __syncthreads();
@@ -117,14 +119,14 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
   const uint32_t lanemask_lt = (1u << lane) - 1u;
 
   for (uint32_t rd = 0; rd < rounds; ++rd) {
-    const uint64_t row0 = ((uint64_t)rd * G + cta) * R;
-    // ---- 1. pass bits and counts per warp segment (segment s * FC_WARPS + w)
+    // this thread's rows of step s: row0 + s * FC_STEP + 4 * lane + c (warp w's segment s * FC_WARPS + w)
+    const uint32_t row0 = (rd * G + cta) * R + w * FC_SEG + 4 * lane;
+    // ---- 1. pass bits and counts per warp segment
     float4 la[FC_DEPTH], tb[FC_DEPTH];
     uint32_t vb[FC_DEPTH];
 #pragma unroll
     for (int d = 0; d < FC_DEPTH; ++d)
-      if ((uint32_t)d < nsteps)
-        load_step(labels, ts, n, row0 + (uint64_t)d * FC_STEP + w * FC_SEG + 4 * lane, la[d], tb[d], vb[d]);
+      if ((uint32_t)d < nsteps) load_step(labels, ts, n, row0 + d * FC_STEP, la[d], tb[d], vb[d]);
     for (uint32_t s0 = 0; s0 < nsteps; s0 += FC_DEPTH) {
 #pragma unroll
       for (int d = 0; d < FC_DEPTH; ++d) {
@@ -132,17 +134,16 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
         if (s < nsteps) {
           const uint32_t seg = s * FC_WARPS + w;
           for (uint32_t p = 0; p < np; ++p) {
-            const uint32_t b4 = pred_bits4(pm[p], la[d], tb[d]) & vb[d];
+            const uint32_t b4 = pred_bits4(pb[p], la[d], tb[d]) & vb[d];
             const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
             const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
             if (lane == 0) {
-              bits[(size_t)p * nseg + seg] = make_uint4(m0, m1, m2, m3);
-              segoff[(size_t)p * nseg + seg] = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+              bits[p * nseg + seg] = make_uint4(m0, m1, m2, m3);
+              segoff[p * nseg + seg] = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
             }
           }
           const uint32_t sn = s + FC_DEPTH;  // the step this slot carries next
-          if (sn < nsteps)
-            load_step(labels, ts, n, row0 + (uint64_t)sn * FC_STEP + w * FC_SEG + 4 * lane, la[d], tb[d], vb[d]);
+          if (sn < nsteps) load_step(labels, ts, n, row0 + sn * FC_STEP, la[d], tb[d], vb[d]);
         }
       }
     }
@@ -151,32 +152,30 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
     for (uint32_t i0 = 0; i0 < nseg; i0 += FC_THREADS) {
       const uint32_t i = i0 + tid;
       for (uint32_t p = 0; p < np; ++p) {
-        const uint32_t v = i < nseg ? segoff[(size_t)p * nseg + i] : 0u;
+        const uint32_t v = i < nseg ? segoff[p * nseg + i] : 0u;
         uint32_t inc = v;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
           const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
           if (lane >= o) inc += x;
         }
-        if (i < nseg) segoff[(size_t)p * nseg + i] = inc - v;  // exclusive within the warp's 32 segments
+        if (i < nseg) segoff[p * nseg + i] = inc - v;  // exclusive within the warp's 32 segments
         if (lane == 31) wtot[p][w] = inc;
       }
       __syncthreads();
       if (tid < (int)np) {  // the warps' totals -> exclusive prefixes, carried across chunks of segments
-        uint32_t acc = 0;
+        const uint64_t carry = i0 ? s_off[tid] : 0u;  // the running total of the earlier chunks
+        uint32_t acc = (uint32_t)carry;
         for (int j = 0; j < FC_WARPS; ++j) {
           const uint32_t x = wtot[tid][j];
           wtot[tid][j] = acc;
           acc += x;
         }
-        // s_off holds the running total of the earlier chunks
-        const uint64_t carry = i0 ? s_off[tid] : 0u;
-        for (int j = 0; j < FC_WARPS; ++j) wtot[tid][j] += (uint32_t)carry;
-        s_off[tid] = carry + acc;
+        s_off[tid] = acc;
       }
       __syncthreads();
       if (i < nseg)
-        for (uint32_t p = 0; p < np; ++p) segoff[(size_t)p * nseg + i] += wtot[p][w];
+        for (uint32_t p = 0; p < np; ++p) segoff[p * nseg + i] += wtot[p][w];
       __syncthreads();
     }
     // the CTA's totals for this round
@@ -199,7 +198,7 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
             f = 1;
             break;
           }
-          __nanosleep(64);
+          __nanosleep(32);
         }
       }
       __threadfence();
@@ -220,10 +219,18 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
     if (w < (int)np) {
       const uint64_t *rp = part + (size_t)(rd & 1) * G * FP_MAXP;
       uint64_t before = 0, all = 0;
-      for (uint32_t c = lane; c < G; c += 32) {
-        const uint64_t x = __ldcg(rp + (size_t)c * FP_MAXP + w);
-        all += x;
-        if (c < cta) before += x;
+      for (uint32_t c0 = 0; c0 < G; c0 += 32 * FC_SUM_UNROLL) {
+        uint64_t x[FC_SUM_UNROLL];
+#pragma unroll
+        for (int j = 0; j < FC_SUM_UNROLL; ++j) {  // the loads first, all in flight
+          const uint32_t c = c0 + j * 32 + lane;
+          x[j] = c < G ? __ldcg(rp + (size_t)c * FP_MAXP + w) : 0ull;
+        }
+#pragma unroll
+        for (int j = 0; j < FC_SUM_UNROLL; ++j) {
+          all += x[j];
+          if (c0 + j * 32 + lane < cta) before += x[j];
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
@@ -236,21 +243,26 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
       }
     }
     __syncthreads();
-    // ---- 4. ids of the passing rows, from the bits
-    for (uint32_t s = 0; s < nsteps; ++s) {
-      const uint32_t seg = s * FC_WARPS + w;
-      const uint64_t r = row0 + (uint64_t)s * FC_STEP + w * FC_SEG + 4 * lane;
-      for (uint32_t p = 0; p < np; ++p) {
-        const uint4 m = bits[(size_t)p * nseg + seg];
+    // ---- 4. ids of the passing rows, from the bits (a segment's bits are
+    // the same for the whole warp, so its skip is uniform)
+    for (uint32_t p = 0; p < np; ++p) {
+      uint32_t *op = out + p * out_stride;
+      const uint32_t base = (uint32_t)s_off[p];
+      const uint4 *bp = bits + p * nseg + w;
+      const uint32_t *sp = segoff + p * nseg + w;
+      for (uint32_t s = 0; s < nsteps; ++s) {
+        const uint4 m = bp[s * FC_WARPS];
+        if ((m.x | m.y | m.z | m.w) == 0u) continue;
         const uint32_t b4 = ((m.x >> lane) & 1u) | (((m.y >> lane) & 1u) << 1) | (((m.z >> lane) & 1u) << 2) |
                             (((m.w >> lane) & 1u) << 3);
-        if (!__any_sync(0xffffffffu, b4)) continue;
-        uint32_t pos = (uint32_t)s_off[p] + segoff[(size_t)p * nseg + seg] + __popc(m.x & lanemask_lt) +
-                       __popc(m.y & lanemask_lt) + __popc(m.z & lanemask_lt) + __popc(m.w & lanemask_lt);
-        uint32_t *op = out + (uint64_t)p * out_stride;
+        if (b4) {
+          uint32_t pos = base + sp[s * FC_WARPS] + __popc(m.x & lanemask_lt) + __popc(m.y & lanemask_lt) +
+                         __popc(m.z & lanemask_lt) + __popc(m.w & lanemask_lt);
+          const uint32_t r = row0 + s * FC_STEP;
 #pragma unroll
-        for (int c = 0; c < 4; ++c)
-          if ((b4 >> c) & 1u) op[pos++] = (uint32_t)(r + c);
+          for (int c = 0; c < 4; ++c)
+            if ((b4 >> c) & 1u) op[pos++] = r + c;
+        }
       }
     }
     __syncthreads();  // bits and offsets are rewritten by the next round
@@ -259,6 +271,51 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
     const bool failed = ld_volatile_u64(flag) == ep;
     counts[tid] = failed ? ~0ull : s_base[tid];
   }
+}
+
+// The floats that int32 truncation maps to v: a closed interval [lo, hi]
+// (empty: lo > hi) — the label test int32(label) == v of utils.h:118 as two
+// float compares.
+void label_interval(int32_t v, float &lo, float &hi) {
+  auto trunc_is = [v](float f) {
+    const double d = std::trunc((double)f);
+    return d >= -2147483648.0 && d < 2147483648.0 && (int64_t)d == (int64_t)v;
+  };
+  const double dv = (double)v;
+  float a, b;
+  if (v > 0) {
+    a = (float)dv;
+    if ((double)a < dv) a = std::nextafter(a, INFINITY);
+    b = (float)(dv + 1.0);
+    while ((double)b >= dv + 1.0) b = std::nextafter(b, -INFINITY);
+  } else if (v < 0) {
+    a = (float)(dv - 1.0);
+    while ((double)a <= dv - 1.0) a = std::nextafter(a, INFINITY);
+    b = (float)dv;
+    if ((double)b > dv) b = std::nextafter(b, -INFINITY);
+  } else {
+    a = std::nextafter(-1.f, INFINITY);
+    b = std::nextafter(1.f, -INFINITY);
+  }
+  if (a <= b && trunc_is(a) && trunc_is(b)) {
+    lo = a;
+    hi = b;
+  } else {
+    lo = INFINITY;
+    hi = -INFINITY;
+  }
+}
+
+// (type, v, l, r) -> the row intervals of FilterPreds (types checked)
+float4 pred_bounds(const float *m) {
+  const int type = (int)m[0];
+  float4 b = make_float4(-INFINITY, INFINITY, -INFINITY, INFINITY);
+  if (type == 1 || type == 3) label_interval((int32_t)m[1], b.x, b.y);
+  if (type == 2 || type == 3) {
+    b.z = m[2];  // NaN bounds pass no row, as the reference's compares
+    b.w = m[3];
+  }
+  return b;
 }
 
 }  // namespace
@@ -324,10 +381,11 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
     std::memset(&P, 0, sizeof(P));
     for (uint32_t p = 0; p < m; ++p) {
       const float *q = metas + (size_t)(p0 + p) * 4;
-      P.m[p] = make_float4(q[0], q[1], q[2], q[3]);
+      P.b[p] = pred_bounds(q);
     }
     const float *lab = idx->labels_f, *tsv = idx->ts_f;
-    uint64_t nn = n, bar_base = fs.arrivals, stride = n;
+    uint32_t nn = (uint32_t)n;
+    uint64_t bar_base = fs.arrivals, stride = n;
     uint32_t mm = m, RR = R, nr = (uint32_t)rounds, ep = ++fs.epoch;
     uint32_t *o = d_out + (uint64_t)p0 * n;
     uint64_t *c = d_counts + p0;
