@@ -372,7 +372,8 @@ typedef struct fknn_router_stats {
   float ms_total;            /* wall time of the call */
   /* wall time of each stage (each ends with its results on the host or in
    * the output): query upload + slabs, SQ8 brute force + re-rank, category
-   * graphs + re-rank, type-0 buckets, type-2 splits, pooled re-rank + copy-out */
+   * graphs + re-rank, the type-0 and type-2 bucket searches (all sub-graphs
+   * side by side), their pool merge on the host, pooled re-rank + copy-out */
   float ms_prepare, ms_bruteforce, ms_category, ms_type0, ms_type2, ms_final;
 } fknn_router_stats;
 

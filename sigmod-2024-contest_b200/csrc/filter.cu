@@ -41,9 +41,10 @@ constexpr int FC_THREADS = 512;
 constexpr int FC_WARPS = FC_THREADS / 32;
 constexpr int FC_STEP = FC_THREADS * 4;  // rows per CTA step: a float4 of each column per thread
 constexpr int FC_SEG = 128;              // rows per warp segment
-constexpr int FC_DEPTH = 4;              // steps in flight per warp
 constexpr uint32_t FP_MAXP = 16;         // predicates per launch
-constexpr size_t FC_SMEM_MAX = 100 * 1024;  // bits + offsets per CTA, so that two CTAs share an SM
+constexpr size_t FC_SMEM_MAX = 104 * 1024;  // ring + bits + offsets per CTA, so that two CTAs share an SM
+constexpr uint32_t FC_STAGE_BYTES = 2 * FC_STEP * 4;  // one ring stage: FC_STEP rows of both columns
+constexpr uint32_t FC_SMAX = 6;                      // ring stages at most
 constexpr int FC_SUM_UNROLL = 10;           // CTA totals in flight per lane (one pass for up to 320 CTAs)
 
 static_assert(FC_WARPS >= (int)FP_MAXP, "one warp per predicate sums the CTA totals");
@@ -89,66 +90,123 @@ __device__ __forceinline__ void load_step(const float *__restrict__ labels, cons
 }
 
 // Grid: G CTAs, all resident.  Rows per CTA per round: R (a multiple of
-// FC_STEP).  Dynamic shared memory: np x nseg x uint4 bits, then np x nseg
+// FC_STEP).  Dynamic shared memory: S ring stages of FC_STEP rows of both
+// columns (bulk copies), then np x nseg x uint4 bits and np x nseg segment
 // offsets (nseg = R / FC_SEG).  sync: [0] the arrival counter (value
 // bar_base at this launch), [1] the failure flag, [2 ..] 2 x G x FP_MAXP
 // per-round CTA totals (double-buffered by round parity).  Row ids fit
 // 32 bits (n < 2^31).
 __global__ void __launch_bounds__(FC_THREADS, 2)
     k_filter_coop(const float *__restrict__ labels, const float *__restrict__ ts, uint32_t n, FilterPreds P,
-                  uint32_t np, uint32_t R, uint32_t rounds, uint64_t *sync, uint64_t bar_base, uint32_t ep,
-                  uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts) {
-  extern __shared__ __align__(16) unsigned char fc_smem[];
-  const uint32_t nseg = R / FC_SEG;
-  uint4 *bits = reinterpret_cast<uint4 *>(fc_smem);                           // [np][nseg]
-  uint32_t *segoff = reinterpret_cast<uint32_t *>(bits + (size_t)np * nseg);  // [np][nseg]
+                  uint32_t np, uint32_t R, uint32_t rounds, uint32_t S, uint64_t *sync, uint64_t bar_base,
+                  uint32_t ep, uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts,
+                  int *err) {
+  extern __shared__ __align__(128) unsigned char fc_smem[];
+  const uint32_t nseg = R / FC_SEG, nchunk = R / FC_STEP;
+  float *ring = reinterpret_cast<float *>(fc_smem);  // stage st: labels [FC_STEP], ts [FC_STEP]
+  uint4 *bits = reinterpret_cast<uint4 *>(fc_smem + (size_t)S * FC_STAGE_BYTES);  // [np][nseg]
+  uint32_t *segoff = reinterpret_cast<uint32_t *>(bits + (size_t)np * nseg);      // [np][nseg]
+  __shared__ uint64_t full[FC_SMAX];
   __shared__ float4 pb[FP_MAXP];
-  __shared__ uint32_t wtot[FP_MAXP][FC_WARPS];
+  __shared__ uint32_t wtot[FP_MAXP][FC_WARPS], wsum[FP_MAXP][FC_WARPS];
   __shared__ uint64_t s_off[FP_MAXP], s_base[FP_MAXP];
   __shared__ int s_fail;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const uint32_t G = gridDim.x, cta = blockIdx.x;
-  const uint32_t nsteps = R / FC_STEP;
   if (tid < (int)FP_MAXP) {
     pb[tid] = P.b[tid];
     s_base[tid] = 0;
+  }
+  if (tid == 0) {
+    for (uint32_t st = 0; st < S; ++st) mbar_init(&full[st], 1);
+    fence_mbar_init();
   }
   __syncthreads();
   unsigned long long *bar = reinterpret_cast<unsigned long long *>(sync);
   uint64_t *flag = sync + 1, *part = sync + 2;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
+  uint32_t phase = 0;  // bit st: the parity of stage st's next completion (the same in every thread)
 
   for (uint32_t rd = 0; rd < rounds; ++rd) {
-    // this thread's rows of step s: row0 + s * FC_STEP + 4 * lane + c (warp w's segment s * FC_WARPS + w)
-    const uint32_t row0 = (rd * G + cta) * R + w * FC_SEG + 4 * lane;
-    // ---- 1. pass bits and counts per warp segment
-    float4 la[FC_DEPTH], tb[FC_DEPTH];
-    uint32_t vb[FC_DEPTH];
-#pragma unroll
-    for (int d = 0; d < FC_DEPTH; ++d)
-      if ((uint32_t)d < nsteps) load_step(labels, ts, n, row0 + d * FC_STEP, la[d], tb[d], vb[d]);
-    for (uint32_t s0 = 0; s0 < nsteps; s0 += FC_DEPTH) {
-#pragma unroll
-      for (int d = 0; d < FC_DEPTH; ++d) {
-        const uint32_t s = s0 + d;
-        if (s < nsteps) {
-          const uint32_t seg = s * FC_WARPS + w;
-          for (uint32_t p = 0; p < np; ++p) {
-            const uint32_t b4 = pred_bits4(pb[p], la[d], tb[d]) & vb[d];
-            const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
-            const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
-            if (lane == 0) {
-              bits[p * nseg + seg] = make_uint4(m0, m1, m2, m3);
-              segoff[p * nseg + seg] = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
-            }
-          }
-          const uint32_t sn = s + FC_DEPTH;  // the step this slot carries next
-          if (sn < nsteps) load_step(labels, ts, n, row0 + sn * FC_STEP, la[d], tb[d], vb[d]);
+    const uint32_t cbase = (rd * G + cta) * R;  // the CTA's first row this round
+    // chunks 0 .. nfull-1 have all their rows and are copied in bulk; the
+    // (one) partial chunk of the base is read by the threads themselves
+    const uint32_t nfull = n > cbase ? min(nchunk, (n - cbase) / FC_STEP) : 0u;
+    auto issue = [&](uint32_t c, uint32_t st) {
+      float *dst = ring + st * (2 * FC_STEP);
+      mbar_arrive_expect_tx(&full[st], FC_STAGE_BYTES);
+      bulk_g2s(dst, labels + cbase + c * FC_STEP, FC_STEP * 4, &full[st]);
+      bulk_g2s(dst + FC_STEP, ts + cbase + c * FC_STEP, FC_STEP * 4, &full[st]);
+    };
+    if (tid == 0)
+      for (uint32_t c = 0; c < S && c < nfull; ++c) issue(c, c);
+    for (uint32_t p = tid; p < np * FC_WARPS; p += FC_THREADS) wsum[p / FC_WARPS][p % FC_WARPS] = 0;
+    __syncthreads();
+    // ---- 1. pass bits per warp segment (segment c * FC_WARPS + w: rows
+    //         cbase + c * FC_STEP + w * FC_SEG + 4 * lane + 0..3)
+    bool gave_up = false;
+    uint32_t c = 0, st = 0;  // chunk, its ring stage (c mod S)
+    const float *mine = ring + w * FC_SEG + 4 * lane;
+    for (; c < nchunk; ++c) {
+      const uint32_t seg = c * FC_WARPS + w;
+      float4 la, tb;
+      uint32_t vb = 0xfu;
+      if (c < nfull) {
+        // warp-uniform: the lanes' timers may disagree at the deadline
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[st], (phase >> st) & 1u, err))) gave_up = true;
+        phase ^= 1u << st;
+        la = *reinterpret_cast<const float4 *>(mine + st * (2 * FC_STEP));
+        tb = *reinterpret_cast<const float4 *>(mine + st * (2 * FC_STEP) + FC_STEP);
+      } else {
+        load_step(labels, ts, n, cbase + c * FC_STEP + w * FC_SEG + 4 * lane, la, tb, vb);
+      }
+      for (uint32_t p = 0; p < np; ++p) {
+        const uint32_t b4 = pred_bits4(pb[p], la, tb) & vb;
+        const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
+        const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
+        if (lane == 0) {
+          const uint32_t cnt = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+          bits[p * nseg + seg] = make_uint4(m0, m1, m2, m3);
+          segoff[p * nseg + seg] = cnt;
+          wsum[p][w] += cnt;
         }
       }
+      // the stage is free once every warp has read it; refill it
+      if (__syncthreads_or(gave_up)) {
+        gave_up = true;
+        break;
+      }
+      if (tid == 0 && c + S < nfull) issue(c + S, st);
+      if (++st == S) st = 0;
     }
-    __syncthreads();
-    // ---- 2. segment offsets inside the CTA (segments in row order), totals
+    if (gave_up) {
+      // a copy did not land in time: wait (bounded) for this CTA's copies
+      // still in flight, flag the launch and poison the counts
+      if (tid == 0) {
+        uint32_t st2 = st;
+        for (uint32_t c2 = c; c2 < c + S && c2 < nfull; ++c2) {
+          const uint32_t par = c2 == c ? (((phase >> st2) & 1u) ^ 1u) : ((phase >> st2) & 1u);
+          mbar_wait_bounded(&full[st2], par, err);
+          if (++st2 == S) st2 = 0;
+        }
+        *(volatile uint64_t *)flag = ep;
+        __threadfence();
+      }
+      __syncthreads();
+      if (tid < (int)np) counts[tid] = ~0ull;
+      return;
+    }
+    // ---- 2. the CTA's totals, published; the barrier arrival (release)
+    if (tid == 0) {
+      uint64_t *mypart = part + ((size_t)(rd & 1) * G + cta) * FP_MAXP;
+      for (uint32_t p = 0; p < np; ++p) {
+        uint32_t t = 0;
+        for (int j = 0; j < FC_WARPS; ++j) t += wsum[p][j];
+        mypart[p] = t;
+      }
+      asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(bar), "l"(1ull) : "memory");
+    }
+    // ---- 3. segment offsets inside the CTA, while the other CTAs finish
     for (uint32_t i0 = 0; i0 < nseg; i0 += FC_THREADS) {
       const uint32_t i = i0 + tid;
       for (uint32_t p = 0; p < np; ++p) {
@@ -164,8 +222,7 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
       }
       __syncthreads();
       if (tid < (int)np) {  // the warps' totals -> exclusive prefixes, carried across chunks of segments
-        const uint64_t carry = i0 ? s_off[tid] : 0u;  // the running total of the earlier chunks
-        uint32_t acc = (uint32_t)carry;
+        uint32_t acc = i0 ? (uint32_t)s_off[tid] : 0u;  // the running total of the earlier chunks
         for (int j = 0; j < FC_WARPS; ++j) {
           const uint32_t x = wtot[tid][j];
           wtot[tid][j] = acc;
@@ -178,35 +235,28 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
         for (uint32_t p = 0; p < np; ++p) segoff[p * nseg + i] += wtot[p][w];
       __syncthreads();
     }
-    // the CTA's totals for this round
-    uint64_t *mypart = part + ((size_t)(rd & 1) * G + cta) * FP_MAXP;
-    if (tid < (int)np) {
-      mypart[tid] = s_off[tid];
-      __threadfence();  // visible to every CTA before this CTA arrives at the barrier
-    }
-    // ---- 3. grid barrier (bounded)
-    __syncthreads();
+    // ---- 4. the grid barrier's wait (bounded, acquire)
     if (tid == 0) {
-      __threadfence();
-      atomicAdd(bar, 1ull);
       const uint64_t target = bar_base + (uint64_t)(rd + 1) * G;
+      auto now = [&]() {
+        uint64_t v;
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+        return v;
+      };
       int f = 0;
-      if (ld_volatile_u64(sync) < target) {
+      if (now() < target) {
         const uint64_t t0 = global_ns();
-        while (ld_volatile_u64(sync) < target) {
+        while (now() < target) {
           if (global_ns() - t0 > WAIT_NS) {
             f = 1;
             break;
           }
-          __nanosleep(32);
         }
       }
-      __threadfence();
       s_fail = f;
     }
     __syncthreads();
     if (s_fail) {
-      // this launch's outputs are incomplete: flag it, poison the counts
       if (tid == 0) {
         *(volatile uint64_t *)flag = ep;
         __threadfence();
@@ -223,8 +273,8 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
         uint64_t x[FC_SUM_UNROLL];
 #pragma unroll
         for (int j = 0; j < FC_SUM_UNROLL; ++j) {  // the loads first, all in flight
-          const uint32_t c = c0 + j * 32 + lane;
-          x[j] = c < G ? __ldcg(rp + (size_t)c * FP_MAXP + w) : 0ull;
+          const uint32_t cc = c0 + j * 32 + lane;
+          x[j] = cc < G ? __ldcg(rp + (size_t)cc * FP_MAXP + w) : 0ull;
         }
 #pragma unroll
         for (int j = 0; j < FC_SUM_UNROLL; ++j) {
@@ -243,29 +293,35 @@ __global__ void __launch_bounds__(FC_THREADS, 2)
       }
     }
     __syncthreads();
-    // ---- 4. ids of the passing rows, from the bits (a segment's bits are
-    // the same for the whole warp, so its skip is uniform)
+    // ---- 5. ids of the passing rows: per segment staged in this warp's
+    //         slice of the (now idle) ring, then stored contiguously
+    uint32_t *stage = reinterpret_cast<uint32_t *>(ring) + w * FC_SEG;
     for (uint32_t p = 0; p < np; ++p) {
       uint32_t *op = out + p * out_stride;
       const uint32_t base = (uint32_t)s_off[p];
       const uint4 *bp = bits + p * nseg + w;
       const uint32_t *sp = segoff + p * nseg + w;
-      for (uint32_t s = 0; s < nsteps; ++s) {
-        const uint4 m = bp[s * FC_WARPS];
-        if ((m.x | m.y | m.z | m.w) == 0u) continue;
+      for (uint32_t cc = 0; cc < nchunk; ++cc) {
+        const uint4 m = bp[cc * FC_WARPS];  // the same for the whole warp: the skip is uniform
+        const uint32_t cnt = __popc(m.x) + __popc(m.y) + __popc(m.z) + __popc(m.w);
+        if (cnt == 0) continue;
         const uint32_t b4 = ((m.x >> lane) & 1u) | (((m.y >> lane) & 1u) << 1) | (((m.z >> lane) & 1u) << 2) |
                             (((m.w >> lane) & 1u) << 3);
-        if (b4) {
-          uint32_t pos = base + sp[s * FC_WARPS] + __popc(m.x & lanemask_lt) + __popc(m.y & lanemask_lt) +
-                         __popc(m.z & lanemask_lt) + __popc(m.w & lanemask_lt);
-          const uint32_t r = row0 + s * FC_STEP;
+        uint32_t k = __popc(m.x & lanemask_lt) + __popc(m.y & lanemask_lt) + __popc(m.z & lanemask_lt) +
+                     __popc(m.w & lanemask_lt);
+        const uint32_t r = cbase + cc * FC_STEP + w * FC_SEG + 4 * lane;
 #pragma unroll
-          for (int c = 0; c < 4; ++c)
-            if ((b4 >> c) & 1u) op[pos++] = r + c;
-        }
+        for (int q = 0; q < 4; ++q)
+          if ((b4 >> q) & 1u) stage[k++] = r + q;
+        __syncwarp();
+        uint32_t *dst = op + base + sp[cc * FC_WARPS];
+        for (uint32_t j = lane; j < cnt; j += 32) dst[j] = stage[j];
+        __syncwarp();  // the slice is rewritten by the next segment
       }
     }
-    __syncthreads();  // bits and offsets are rewritten by the next round
+    // the ring's generic writes before the next round's bulk copies into it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();  // bits, offsets and the ring are rewritten by the next round
   }
   if (cta == 0 && tid < (int)np) {
     const bool failed = ld_volatile_u64(flag) == ep;
@@ -370,13 +426,26 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
   }
   for (uint32_t p0 = 0; p0 < np; p0 += FP_MAXP) {
     const uint32_t m = std::min<uint32_t>(FP_MAXP, np - p0);
-    // rows per CTA per round: as few rounds as the bits allow, rows split evenly
-    const size_t per_row = (size_t)m * (sizeof(uint4) + sizeof(uint32_t));  // per 128-row segment
-    const uint64_t r_cap = std::max<uint64_t>(FC_STEP, (FC_SMEM_MAX / per_row) * FC_SEG / FC_STEP * FC_STEP);
-    const uint64_t rounds = std::max<uint64_t>(1, (n + (uint64_t)G * r_cap - 1) / ((uint64_t)G * r_cap));
-    const uint64_t per_cta = (n + (uint64_t)G * rounds - 1) / ((uint64_t)G * rounds);
-    const uint32_t R = (uint32_t)std::max<uint64_t>(FC_STEP, (per_cta + FC_STEP - 1) / FC_STEP * FC_STEP);
-    const size_t smem = (size_t)(R / FC_SEG) * per_row;
+    // rows per CTA per round and ring stages: one round with the deepest
+    // ring the shared memory leaves room for, else two stages and as few
+    // rounds as the bits allow (rows split evenly)
+    const size_t per_seg = (size_t)m * (sizeof(uint4) + sizeof(uint32_t));  // bits + offset per 128 rows
+    const uint64_t one = ((n + G - 1) / G + FC_STEP - 1) / FC_STEP * FC_STEP;
+    uint32_t S;
+    uint64_t rounds, R;
+    if ((one / FC_SEG) * per_seg + 2 * FC_STAGE_BYTES <= FC_SMEM_MAX) {
+      rounds = 1;
+      R = one;
+      S = (uint32_t)std::min<size_t>(FC_SMAX, (FC_SMEM_MAX - (one / FC_SEG) * per_seg) / FC_STAGE_BYTES);
+    } else {
+      S = 2;
+      const uint64_t r_cap = std::max<uint64_t>(
+          FC_STEP, ((FC_SMEM_MAX - 2 * FC_STAGE_BYTES) / per_seg) * FC_SEG / FC_STEP * FC_STEP);
+      rounds = (n + G * r_cap - 1) / (G * r_cap);
+      const uint64_t per_cta = (n + G * rounds - 1) / (G * rounds);
+      R = std::max<uint64_t>(FC_STEP, (per_cta + FC_STEP - 1) / FC_STEP * FC_STEP);
+    }
+    const size_t smem = (size_t)S * FC_STAGE_BYTES + (size_t)(R / FC_SEG) * per_seg;
     FilterPreds P;
     std::memset(&P, 0, sizeof(P));
     for (uint32_t p = 0; p < m; ++p) {
@@ -386,11 +455,13 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
     const float *lab = idx->labels_f, *tsv = idx->ts_f;
     uint32_t nn = (uint32_t)n;
     uint64_t bar_base = fs.arrivals, stride = n;
-    uint32_t mm = m, RR = R, nr = (uint32_t)rounds, ep = ++fs.epoch;
+    uint32_t mm = m, RR = (uint32_t)R, nr = (uint32_t)rounds, SS = S, ep = ++fs.epoch;
     uint32_t *o = d_out + (uint64_t)p0 * n;
     uint64_t *c = d_counts + p0;
+    int *errp = idx->d_flag;
     void *args[] = {(void *)&lab, (void *)&tsv, (void *)&nn, (void *)&P, (void *)&mm, (void *)&RR, (void *)&nr,
-                    (void *)&sync, (void *)&bar_base, (void *)&ep, (void *)&o, (void *)&stride, (void *)&c};
+                    (void *)&SS, (void *)&sync, (void *)&bar_base, (void *)&ep, (void *)&o, (void *)&stride,
+                    (void *)&c, (void *)&errp};
     FKNN_CUDA(cudaLaunchCooperativeKernel((const void *)k_filter_coop, dim3(G), dim3(FC_THREADS), args, smem, st));
     fs.arrivals += rounds * G;
     g_launches += 1;

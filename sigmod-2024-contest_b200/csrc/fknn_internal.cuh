@@ -327,6 +327,18 @@ int device_plan_build(fknn_index *idx, const QueryDesc *d_desc, const float *d_m
 int search_exact(fknn_index *idx, const float *d_q, const float *d_meta, uint32_t nq, uint32_t k, uint32_t *d_ids,
                  float *d_dists, cudaStream_t st, fknn_search_stats *stats);
 int count_matches(fknn_index *idx, const float *d_meta, uint32_t nq, uint32_t *d_counts, cudaStream_t st);
+// graph search (graph_search.cu) without a host round trip: checked
+// arguments, device inputs and outputs; the graph's error flag collects
+// the searches enqueued since graph_flag_reset
+int graph_check_args(const fknn_graph *g, const float *queries, uint32_t nq, int mode, uint32_t k, uint32_t ef,
+                     uint32_t refine, const float *bounds, const int32_t *id_bounds, const int32_t *out_ids,
+                     uint32_t *cap);
+int graph_reserve(fknn_graph *g, uint32_t nq, uint32_t cap);
+int graph_launch(fknn_graph *g, const float *d_q, uint32_t nq, int mode, uint32_t k, uint32_t cap, uint32_t refine,
+                 const float *d_bounds, const int32_t *d_idb, int32_t *d_ids, float *d_dists, cudaStream_t st);
+int graph_flag_reset(fknn_graph *g, cudaStream_t st);
+int graph_flag_check(fknn_graph *g);
+
 // predicate compaction (filter.cu): host predicates, device outputs
 int filter_check_preds(const float *metas_host, uint32_t np, const char *who);
 int filter_rows_batch(fknn_index *idx, const float *metas_host, uint32_t np, uint32_t *d_out, uint64_t *d_counts,

@@ -610,6 +610,142 @@ bool parse_graph(const unsigned char *b, size_t nbytes, HostGraph &h) {
 
 using namespace fknn;
 
+namespace fknn {
+
+// The argument checks of fknn_graph_search; *cap = the pool capacity.
+int graph_check_args(const fknn_graph *g, const float *queries, uint32_t nq, int mode, uint32_t k, uint32_t ef,
+                     uint32_t refine, const float *bounds, const int32_t *id_bounds, const int32_t *out_ids,
+                     uint32_t *cap) {
+  (void)nq;
+  if (!g || !queries || !out_ids) {
+    set_error("fknn_graph_search: NULL argument");
+    return FKNN_EINVAL;
+  }
+  if (mode < FKNN_GRAPH_SEARCH || mode > FKNN_GRAPH_RANGE) {
+    set_error("fknn_graph_search: unknown mode");
+    return FKNN_EINVAL;
+  }
+  if (ef == 0) ef = EF_DEFAULT;
+  *cap = std::max(k, ef);  // LinearPool(nb, max(k, ef), k)
+  if (k == 0 || *cap > CAP_MAX || refine == 0 || refine > *cap + 1) {
+    set_error("fknn_graph_search: need 1 <= k, max(k, ef) <= 4096 and 1 <= refine <= max(k, ef) + 1");
+    return FKNN_EINVAL;
+  }
+  if (mode == FKNN_GRAPH_SEARCH && refine != k) {
+    set_error("fknn_graph_search: mode 0 (Search) writes k ids; refine must equal k");
+    return FKNN_EINVAL;
+  }
+  if (mode >= FKNN_GRAPH_CATEGORY_RANGE && (!bounds || !id_bounds)) {
+    set_error("fknn_graph_search: modes 3-5 need bounds and id_bounds");
+    return FKNN_EINVAL;
+  }
+  return FKNN_OK;
+}
+
+// Launch geometry of a search of nq queries at pool capacity cap.
+static int graph_geometry(const fknn_graph *g, uint32_t nq, uint32_t cap, size_t *smem, size_t *grid,
+                          uint32_t *nwords, uint32_t *nblkw) {
+  const uint32_t nblocks512 = (g->n + 511) / 512;
+  *nwords = nblocks512 * 8;
+  *nblkw = (nblocks512 + 31) / 32;
+  *smem = warp_smem_bytes(cap, *nblkw) * GS_WARPS;
+  if (*smem > 200 * 1024) {
+    set_error("fknn_graph_search: pool and visited flags exceed shared memory (max(k, ef) or n too large)");
+    return FKNN_EINVAL;
+  }
+  FKNN_CUDA(cudaFuncSetAttribute(k_graph_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)*smem));
+  int per_sm = 0;
+  FKNN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_graph_search, GS_WARPS * 32, *smem));
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
+  const size_t slot_bytes = (size_t)*nwords * 16;
+  const size_t max_slots = std::max<size_t>(GS_WARPS, VIS_BUDGET / slot_bytes);
+  size_t gr = (size_t)sms * std::max(per_sm, 1);
+  gr = std::min(gr, std::max<size_t>(1, max_slots / GS_WARPS));
+  *grid = std::min(gr, ((size_t)nq + GS_WARPS - 1) / GS_WARPS);
+  return FKNN_OK;
+}
+
+// Grows the graph's per-call scratch for searches of up to nq queries at
+// pool capacity up to cap, so that graph_launch allocates nothing.
+int graph_reserve(fknn_graph *g, uint32_t nq, uint32_t cap) {
+  size_t smem, grid;
+  uint32_t nwords, nblkw;
+  int rc;
+  if ((rc = graph_geometry(g, nq, cap, &smem, &grid, &nwords, &nblkw))) return rc;
+  if ((rc = grow(&g->qcodes, &g->qcodes_cap, (size_t)nq * CODE))) return rc;
+  return grow(&g->vis, &g->vis_cap, grid * GS_WARPS * 2 * (size_t)nwords);
+}
+
+// Enqueues one search on st (device inputs and outputs, checked arguments);
+// the graph's error flag accumulates until graph_flag_reset.
+int graph_launch(fknn_graph *g, const float *q_use, uint32_t nq, int mode, uint32_t k, uint32_t cap,
+                 uint32_t refine, const float *b_use, const int32_t *ib_use, int32_t *ids_use, float *d_use,
+                 cudaStream_t st) {
+  int rc;
+  if ((rc = grow(&g->qcodes, &g->qcodes_cap, (size_t)nq * CODE))) return rc;
+  launch_sq8_encode(q_use, nq, g->alpha, g->qcodes, st);
+  size_t smem, grid;
+  uint32_t nwords, nblkw;
+  if ((rc = graph_geometry(g, nq, cap, &smem, &grid, &nwords, &nblkw))) return rc;
+  if ((rc = grow(&g->vis, &g->vis_cap, grid * GS_WARPS * 2 * (size_t)nwords))) return rc;
+  const bool ranged = mode >= FKNN_GRAPH_CATEGORY_RANGE;
+  GParams P;
+  P.adj = g->adj;
+  P.ets = g->ets;
+  P.levels = g->levels;
+  P.up_off = g->up_off;
+  P.up = g->up;
+  P.eps = g->eps;
+  P.codes = g->codes;
+  P.n = g->n;
+  P.K = g->K;
+  P.upK = g->upK;
+  P.nep = g->nep;
+  P.ep = g->ep;
+  P.alpha2 = g->alpha * g->alpha;
+  P.qcodes = g->qcodes;
+  P.nq = nq;
+  P.mode = mode;
+  P.cap = cap;
+  P.refine = refine;
+  P.batch = refine <= cap;
+  P.bounds = ranged ? b_use : nullptr;
+  P.id_bounds = ranged ? ib_use : nullptr;
+  P.out_ids = ids_use;
+  P.out_dists = d_use;
+  P.vis = g->vis;
+  P.nwords = nwords;
+  P.nblkw = nblkw;
+  P.err = g->dflag;
+  k_graph_search<<<(unsigned)grid, GS_WARPS * 32, smem, st>>>(P);
+  g_launches += 1;
+  FKNN_CUDA(cudaGetLastError());
+  return FKNN_OK;
+}
+
+int graph_flag_reset(fknn_graph *g, cudaStream_t st) {
+  FKNN_CUDA(cudaMemsetAsync(g->dflag, 0, 4, st));
+  return FKNN_OK;
+}
+
+// The searches enqueued since the last reset (call after they finished).
+int graph_flag_check(fknn_graph *g) {
+  int flag = 0;
+  FKNN_CUDA(cudaMemcpy(&flag, g->dflag, 4, cudaMemcpyDeviceToHost));
+  if (flag & ERR_BAD_QUERY_VALUE) {
+    set_error("fknn_graph_search: id_bounds seed a point outside [0, n)");
+    return FKNN_EINVAL;
+  }
+  if (flag) {
+    set_error("fknn_graph_search: a search exceeded its pop bound");
+    return FKNN_ETIMEOUT;
+  }
+  return FKNN_OK;
+}
+
+}  // namespace fknn
+
 extern "C" {
 
 int fknn_graph_create(const void *graph_bytes, size_t nbytes, const float *vecs, int device, fknn_graph **out) {
@@ -693,36 +829,16 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
                       uint32_t refine, const float *bounds, const int32_t *id_bounds, int32_t *out_ids,
                       float *out_dists, void *stream) {
   g_launches = 0;
-  if (!g || !queries || !out_ids) {
-    set_error("fknn_graph_search: NULL argument");
-    return FKNN_EINVAL;
-  }
-  if (mode < FKNN_GRAPH_SEARCH || mode > FKNN_GRAPH_RANGE) {
-    set_error("fknn_graph_search: unknown mode");
-    return FKNN_EINVAL;
-  }
-  if (ef == 0) ef = EF_DEFAULT;
-  const uint32_t cap = std::max(k, ef);  // LinearPool(nb, max(k, ef), k)
-  if (k == 0 || cap > CAP_MAX || refine == 0 || refine > cap + 1) {
-    set_error("fknn_graph_search: need 1 <= k, max(k, ef) <= 4096 and 1 <= refine <= max(k, ef) + 1");
-    return FKNN_EINVAL;
-  }
-  if (mode == FKNN_GRAPH_SEARCH && refine != k) {
-    set_error("fknn_graph_search: mode 0 (Search) writes k ids; refine must equal k");
-    return FKNN_EINVAL;
-  }
-  const bool ranged = mode >= FKNN_GRAPH_CATEGORY_RANGE;
-  if (ranged && (!bounds || !id_bounds)) {
-    set_error("fknn_graph_search: modes 3-5 need bounds and id_bounds");
-    return FKNN_EINVAL;
-  }
+  uint32_t cap = 0;
+  int rc;
+  if ((rc = fknn::graph_check_args(g, queries, nq, mode, k, ef, refine, bounds, id_bounds, out_ids, &cap))) return rc;
   if (nq == 0) return FKNN_OK;
   FKNN_CUDA(cudaSetDevice(g->device));
   cudaStream_t st = (cudaStream_t)stream;
+  const bool ranged = mode >= FKNN_GRAPH_CATEGORY_RANGE;
 
   // staging: [queries | bounds | id_bounds | ids | dists], 4-byte words
   const size_t qf = (size_t)nq * DIM, bf = ranged ? (size_t)nq * 2 : 0, of = (size_t)nq * refine;
-  int rc;
   if ((rc = grow(&g->io, &g->io_cap, qf + 2 * bf + 2 * of))) return rc;
   float *s_q = g->io, *s_b = s_q + qf;
   int32_t *s_ib = reinterpret_cast<int32_t *>(s_b + bf);
@@ -745,76 +861,13 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
   }
   int32_t *ids_use = on_device(out_ids) ? out_ids : s_ids;
   float *d_use = out_dists ? (on_device(out_dists) ? out_dists : s_d) : nullptr;
-
-  if ((rc = grow(&g->qcodes, &g->qcodes_cap, (size_t)nq * CODE))) return rc;
-  launch_sq8_encode(q_use, nq, g->alpha, g->qcodes, st);
-
-  const uint32_t nblocks512 = (g->n + 511) / 512;
-  const uint32_t nwords = nblocks512 * 8, nblkw = (nblocks512 + 31) / 32;
-  const size_t smem = warp_smem_bytes(cap, nblkw) * GS_WARPS;
-  if (smem > 200 * 1024) {
-    set_error("fknn_graph_search: pool and visited flags exceed shared memory (max(k, ef) or n too large)");
-    return FKNN_EINVAL;
-  }
-  FKNN_CUDA(cudaFuncSetAttribute(k_graph_search, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  int per_sm = 0;
-  FKNN_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_graph_search, GS_WARPS * 32, smem));
-  int sms = 148;
-  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, g->device);
-  const size_t slot_bytes = (size_t)nwords * 16;
-  const size_t max_slots = std::max<size_t>(GS_WARPS, VIS_BUDGET / slot_bytes);
-  size_t grid = (size_t)sms * std::max(per_sm, 1);
-  grid = std::min(grid, std::max<size_t>(1, max_slots / GS_WARPS));
-  grid = std::min(grid, ((size_t)nq + GS_WARPS - 1) / GS_WARPS);
-  if ((rc = grow(&g->vis, &g->vis_cap, grid * GS_WARPS * 2 * (size_t)nwords))) return rc;
   FKNN_CUDA(cudaMemsetAsync(g->dflag, 0, 4, st));
-
-  GParams P;
-  P.adj = g->adj;
-  P.ets = g->ets;
-  P.levels = g->levels;
-  P.up_off = g->up_off;
-  P.up = g->up;
-  P.eps = g->eps;
-  P.codes = g->codes;
-  P.n = g->n;
-  P.K = g->K;
-  P.upK = g->upK;
-  P.nep = g->nep;
-  P.ep = g->ep;
-  P.alpha2 = g->alpha * g->alpha;
-  P.qcodes = g->qcodes;
-  P.nq = nq;
-  P.mode = mode;
-  P.cap = cap;
-  P.refine = refine;
-  P.batch = refine <= cap;
-  P.bounds = ranged ? b_use : nullptr;
-  P.id_bounds = ranged ? ib_use : nullptr;
-  P.out_ids = ids_use;
-  P.out_dists = d_use;
-  P.vis = g->vis;
-  P.nwords = nwords;
-  P.nblkw = nblkw;
-  P.err = g->dflag;
-  k_graph_search<<<(unsigned)grid, GS_WARPS * 32, smem, st>>>(P);
-  g_launches += 1;
-  FKNN_CUDA(cudaGetLastError());
+  if ((rc = fknn::graph_launch(g, q_use, nq, mode, k, cap, refine, b_use, ib_use, ids_use, d_use, st))) return rc;
   if (ids_use != out_ids) FKNN_CUDA(cudaMemcpyAsync(out_ids, ids_use, of * 4, cudaMemcpyDeviceToHost, st));
   if (out_dists && d_use != out_dists)
     FKNN_CUDA(cudaMemcpyAsync(out_dists, d_use, of * 4, cudaMemcpyDeviceToHost, st));
-  int flag = 0;
-  FKNN_CUDA(cudaMemcpyAsync(&flag, g->dflag, 4, cudaMemcpyDeviceToHost, st));
   FKNN_CUDA(cudaStreamSynchronize(st));
-  if (flag & ERR_BAD_QUERY_VALUE) {
-    set_error("fknn_graph_search: id_bounds seed a point outside [0, n)");
-    return FKNN_EINVAL;
-  }
-  if (flag) {
-    set_error("fknn_graph_search: a search exceeded its pop bound");
-    return FKNN_ETIMEOUT;
-  }
-  return FKNN_OK;
+  return fknn::graph_flag_check(g);
 }
 
 }  // extern "C"

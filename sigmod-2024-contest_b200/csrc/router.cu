@@ -28,6 +28,7 @@
 #include <chrono>
 #include <cmath>
 #include <cstring>
+#include <deque>
 #include <vector>
 
 #include "device_util.cuh"
@@ -230,6 +231,9 @@ struct fknn_router {
   int device = 0;
   fknn_index *idx = nullptr;
   cudaStream_t st = nullptr;
+  std::vector<cudaStream_t> sst;             // one per sub-graph (categories, then buckets)
+  std::vector<cudaEvent_t> sev;              // their joins
+  cudaEvent_t ev_in = nullptr;               // a stage's inputs are staged
   float alpha = 0.f;                         // SQ8 scale over the whole base (the full searcher's)
   int8_t *codes[2] = {nullptr, nullptr};     // SQ8 codes in the index's ORDER_TIME / ORDER_CAT row orders
   uint32_t *d_cat_ids = nullptr, *d_full_ids = nullptr;
@@ -266,6 +270,11 @@ void destroy_router(fknn_router *r) {
   cudaFree(r->d_cat_ids);
   cudaFree(r->d_full_ids);
   if (r->st) cudaStreamDestroy(r->st);
+  for (cudaStream_t x : r->sst)
+    if (x) cudaStreamDestroy(x);
+  for (cudaEvent_t x : r->sev)
+    if (x) cudaEventDestroy(x);
+  if (r->ev_in) cudaEventDestroy(r->ev_in);
   delete r;
 }
 
@@ -294,11 +303,6 @@ int add_subgraphs(fknn_router *r, const fknn_router_subgraph *sg, uint32_t nsg, 
     }
   }
   return FKNN_OK;
-}
-
-int launch_graph(fknn_router *r, const fknn_router::Sub &sub, int mode, const float *d_q, uint32_t nq, uint32_t K,
-                 uint32_t refine, const float *d_bounds, const int32_t *d_idb, int32_t *d_ids, float *d_d) {
-  return fknn_graph_search(sub.g, d_q, nq, mode, K, 0, refine, d_bounds, d_idb, d_ids, d_d, r->st);
 }
 
 }  // namespace
@@ -391,6 +395,16 @@ int fknn_router_create(const fknn_router_desc *d, fknn_router **out) {
   if ((rc = add_subgraphs(r, d->buckets, d->nbuckets, d->sorted_base_ids_by_full_time, d->vecs, n, r->bks,
                           "time-bucket")))
     return fail(rc);
+  // the sub-graphs' searches of a stage run side by side
+  const size_t nsub = r->cats.size() + r->bks.size();
+  r->sst.assign(nsub, nullptr);
+  r->sev.assign(nsub, nullptr);
+  cudaError_t e2 = cudaEventCreateWithFlags(&r->ev_in, cudaEventDisableTiming);
+  for (size_t i = 0; i < nsub && e2 == cudaSuccess; ++i) {
+    e2 = cudaStreamCreateWithFlags(&r->sst[i], cudaStreamNonBlocking);
+    if (e2 == cudaSuccess) e2 = cudaEventCreateWithFlags(&r->sev[i], cudaEventDisableTiming);
+  }
+  if (e2 != cudaSuccess) return fail(cuda_fail(e2, "fknn_router_create"));
   *out = r;
   return FKNN_OK;
 }
@@ -492,16 +506,6 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
     FKNN_CUDA(cudaStreamSynchronize(st));  // list and the staging buffers are reused next
     return FKNN_OK;
   };
-  // the queries of `list` gathered into r->qsub (graph searches take them contiguous)
-  auto gather_queries = [&](const std::vector<uint32_t> &list) -> int {
-    const uint32_t m = (uint32_t)list.size();
-    int rc2;
-    if ((rc2 = r->rows.get(m)) || (rc2 = r->qsub.get((size_t)m * DIM))) return rc2;
-    FKNN_CUDA(cudaMemcpyAsync(r->rows.p, list.data(), (size_t)m * 4, cudaMemcpyHostToDevice, st));
-    k_gather_rows<<<grid_of((uint64_t)m * DIM), 256, 0, st>>>(r->q.p, r->rows.p, m, DIM, r->qsub.p);
-    g_launches += 1;
-    return FKNN_OK;
-  };
 
   // 1. brute force over the slab with the global codes, FP32 re-rank of
   //    the bf_refine_k candidates (hybrid_graph.cpp:201-229)
@@ -531,172 +535,337 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
   }
   S.ms_bruteforce = lap();
 
+  // The graph searches of a stage, enqueued together: every sub-graph's
+  // searches on that sub-graph's stream (one graph's scratch serves one
+  // search at a time), all inputs staged by one copy each, all outputs read
+  // back once.  Batches keep the reference's order, in which their
+  // candidates are merged afterwards.
+  struct GBatch {
+    uint32_t sub;                         // index into subs()
+    int mode;
+    const std::vector<uint32_t> *list;
+    uint32_t K;                           // pool argument of the search
+    std::vector<float> hb;                // ranged forms: the windows ...
+    std::vector<int32_t> hib;             // ... and their row ranges in the sub-graph
+    bool dists;
+    size_t q0 = 0, b0 = 0, o0 = 0;        // offsets: queries, windows, outputs
+  };
+  struct BBatch {                         // SQ8 brute force over a bucket's own codes (SplitInterval SMALL)
+    uint32_t sub;
+    std::vector<uint32_t> list, s, cnt;
+    size_t q0 = 0, k0 = 0;
+  };
+  auto subs = [&](uint32_t i) -> const fknn_router::Sub & {
+    return i < r->cats.size() ? r->cats[i] : r->bks[i - r->cats.size()];
+  };
+  std::vector<int32_t> h_ids;
+  std::vector<float> h_d;
+  std::vector<uint64_t> h_keys;
+  auto run_stage = [&](std::vector<GBatch> &B, std::vector<BBatch> &BB, bool to_host) -> int {
+    size_t nqs = 0, nb = 0, no = 0, nk = 0;
+    const uint32_t kb = P.bf_refine_k;
+    std::vector<uint32_t> rows;
+    std::vector<float> hb;
+    std::vector<int32_t> hib;
+    std::vector<uint32_t> hsel;
+    for (GBatch &b : B) {
+      b.q0 = nqs;
+      b.b0 = nb;
+      b.o0 = no;
+      rows.insert(rows.end(), b.list->begin(), b.list->end());
+      nqs += b.list->size();
+      no += b.list->size() * R;
+      if (!b.hb.empty()) {
+        hb.insert(hb.end(), b.hb.begin(), b.hb.end());
+        hib.insert(hib.end(), b.hib.begin(), b.hib.end());
+        nb += b.list->size();
+      }
+    }
+    for (BBatch &b : BB) {
+      b.q0 = nqs;
+      b.k0 = nk;
+      for (size_t j = 0; j < b.list.size(); ++j) {
+        hsel.push_back((uint32_t)(b.q0 + j));  // the query's row in the staged queries
+        hsel.push_back(b.s[j]);
+        hsel.push_back(b.s[j] + b.cnt[j]);
+      }
+      rows.insert(rows.end(), b.list.begin(), b.list.end());
+      nqs += b.list.size();
+      nk += b.list.size() * kb;
+    }
+    if (!nqs) return FKNN_OK;
+    int rc2;
+    if ((rc2 = r->rows.get(nqs)) || (rc2 = r->qsub.get(nqs * DIM)) || (rc2 = r->bounds.get(std::max<size_t>(nb, 1) * 2)) ||
+        (rc2 = r->idb.get(std::max<size_t>(nb, 1) * 2)) || (rc2 = r->lids.get(std::max<size_t>(no, 1))) ||
+        (rc2 = r->ldist.get(std::max<size_t>(no, 1))) || (rc2 = r->qcodes_b.get(nqs * CODE)) ||
+        (rc2 = r->sel.get(std::max<size_t>(hsel.size(), 3))) || (rc2 = r->keys.get(std::max<size_t>(nk, 1))))
+      return rc2;
+    // scratch of every graph at its largest search of the stage (nothing is
+    // allocated once searches are in flight)
+    std::vector<uint32_t> used;
+    {
+      std::vector<uint32_t> mq(r->cats.size() + r->bks.size(), 0), mc(mq.size(), 0);
+      for (GBatch &b : B) {
+        uint32_t cap = 0;
+        if ((rc2 = graph_check_args(subs(b.sub).g, r->q.p, (uint32_t)b.list->size(), b.mode, b.K, 0, R, r->bounds.p,
+                                    r->idb.p, r->lids.p, &cap)))
+          return rc2;
+        mq[b.sub] = std::max<uint32_t>(mq[b.sub], (uint32_t)b.list->size());
+        mc[b.sub] = std::max(mc[b.sub], cap);
+      }
+      for (uint32_t i = 0; i < mq.size(); ++i)
+        if (mq[i]) {
+          used.push_back(i);
+          if ((rc2 = graph_reserve(subs(i).g, mq[i], mc[i]))) return rc2;
+        }
+    }
+    FKNN_CUDA(cudaMemcpyAsync(r->rows.p, rows.data(), nqs * 4, cudaMemcpyHostToDevice, st));
+    if (nb) {
+      FKNN_CUDA(cudaMemcpyAsync(r->bounds.p, hb.data(), nb * 8, cudaMemcpyHostToDevice, st));
+      FKNN_CUDA(cudaMemcpyAsync(r->idb.p, hib.data(), nb * 8, cudaMemcpyHostToDevice, st));
+    }
+    if (!hsel.empty()) FKNN_CUDA(cudaMemcpyAsync(r->sel.p, hsel.data(), hsel.size() * 4, cudaMemcpyHostToDevice, st));
+    k_gather_rows<<<grid_of((uint64_t)nqs * DIM), 256, 0, st>>>(r->q.p, r->rows.p, (uint32_t)nqs, DIM, r->qsub.p);
+    g_launches += 1;
+    FKNN_CUDA(cudaEventRecord(r->ev_in, st));
+    std::vector<uint8_t> waiting(r->sst.size(), 0);
+    auto join_in = [&](uint32_t i) -> int {
+      if (!waiting[i]) {
+        FKNN_CUDA(cudaStreamWaitEvent(r->sst[i], r->ev_in, 0));
+        waiting[i] = 1;
+      }
+      return FKNN_OK;
+    };
+    for (uint32_t i : used) {
+      if ((rc2 = join_in(i))) return rc2;
+      if ((rc2 = graph_flag_reset(subs(i).g, r->sst[i]))) return rc2;
+    }
+    for (GBatch &b : B) {
+      const uint32_t m = (uint32_t)b.list->size();
+      if (!m) continue;
+      uint32_t cap = 0;
+      graph_check_args(subs(b.sub).g, r->q.p, m, b.mode, b.K, 0, R, r->bounds.p, r->idb.p, r->lids.p, &cap);
+      const bool ranged = !b.hb.empty();
+      if ((rc2 = graph_launch(subs(b.sub).g, r->qsub.p + b.q0 * DIM, m, b.mode, b.K, cap, R,
+                              ranged ? r->bounds.p + 2 * b.b0 : nullptr, ranged ? r->idb.p + 2 * b.b0 : nullptr,
+                              r->lids.p + b.o0, b.dists ? r->ldist.p + b.o0 : nullptr, r->sst[b.sub])))
+        return rc2;
+      ++S.n_graph_calls;
+    }
+    for (BBatch &b : BB) {
+      const uint32_t m = (uint32_t)b.list.size();
+      const int8_t *bcodes;
+      float ba;
+      uint32_t bn;
+      graph_codes(subs(b.sub).g, &bcodes, &ba, &bn);
+      if ((rc2 = join_in(b.sub))) return rc2;
+      launch_sq8_encode(r->qsub.p + b.q0 * DIM, m, ba, r->qcodes_b.p + b.q0 * CODE, r->sst[b.sub]);
+      // sel rows name the query's row in the staged queries, codes_b holds them at the same rows
+      k_sq8_slab_topk<<<std::min<uint32_t>(m, 148 * 8), ST_THREADS, 0, r->sst[b.sub]>>>(
+          bcodes, bcodes, r->qcodes_b.p, r->sel.p + 3 * (b.k0 / kb), nullptr, m, kb, r->keys.p + b.k0);
+      g_launches += 2;
+    }
+    for (uint32_t i = 0; i < r->sst.size(); ++i)
+      if (waiting[i]) {
+        FKNN_CUDA(cudaEventRecord(r->sev[i], r->sst[i]));
+        FKNN_CUDA(cudaStreamWaitEvent(st, r->sev[i], 0));
+      }
+    if (to_host) {
+      h_ids.resize(no);
+      h_d.resize(no);
+      h_keys.resize(nk);
+      if (no) {
+        FKNN_CUDA(cudaMemcpyAsync(h_ids.data(), r->lids.p, no * 4, cudaMemcpyDeviceToHost, st));
+        FKNN_CUDA(cudaMemcpyAsync(h_d.data(), r->ldist.p, no * 4, cudaMemcpyDeviceToHost, st));
+      }
+      if (nk) FKNN_CUDA(cudaMemcpyAsync(h_keys.data(), r->keys.p, nk * 8, cudaMemcpyDeviceToHost, st));
+    }
+    FKNN_CUDA(cudaStreamSynchronize(st));
+    for (uint32_t i : used)
+      if ((rc2 = graph_flag_check(subs(i).g))) return rc2;
+    return FKNN_OK;
+  };
+
   // 2. category graphs (hybrid_graph.cpp:239-298): pool ceil(ef_min +
   //    slope * category size), graph_refine_k candidates, FP32 re-rank
-  for (size_t c = 0; c < r->cats.size(); ++c) {
-    const fknn_router::Sub &sub = r->cats[c];
-    for (int form = 0; form < 2; ++form) {
-      const std::vector<uint32_t> &list = form == 0 ? cat1[c] : cat3[c];
-      const uint32_t m = (uint32_t)list.size();
-      if (!m) continue;
-      const uint32_t Kp = form == 0 ? (uint32_t)std::ceil((float)P.ef1min + slope1 * (float)sub.count)
-                                    : (uint32_t)std::ceil((float)P.ef3min + slope3 * (float)sub.count);
-      if ((rc = gather_queries(list)) || (rc = r->lids.get((size_t)m * R)) || (rc = r->cand.get((size_t)m * R)))
-        return rc;
-      if (form == 0) {
-        rc = launch_graph(r, sub, FKNN_GRAPH_FILTER, r->qsub.p, m, Kp, R, nullptr, nullptr, r->lids.p, nullptr);
-      } else {
-        // the window (l, r) and the slab's positions inside the category (:275-282)
-        std::vector<float> hb((size_t)m * 2);
-        std::vector<int32_t> hib((size_t)m * 2);
-        for (uint32_t j = 0; j < m; ++j) {
-          const float *mt = metas + (size_t)list[j] * 4;
-          hb[2 * j] = mt[2];
-          hb[2 * j + 1] = mt[3];
-          hib[2 * j] = (int32_t)(h_desc[list[j]].s - sub.start);
-          hib[2 * j + 1] = (int32_t)(h_desc[list[j]].e - sub.start);
+  {
+    std::vector<GBatch> B;
+    std::vector<BBatch> none;
+    for (size_t c = 0; c < r->cats.size(); ++c) {
+      const fknn_router::Sub &sub = r->cats[c];
+      for (int form = 0; form < 2; ++form) {
+        const std::vector<uint32_t> &list = form == 0 ? cat1[c] : cat3[c];
+        const uint32_t m = (uint32_t)list.size();
+        if (!m) continue;
+        GBatch b;
+        b.sub = (uint32_t)c;
+        b.mode = form == 0 ? FKNN_GRAPH_FILTER : FKNN_GRAPH_CATEGORY_RANGE;
+        b.list = &list;
+        b.K = form == 0 ? (uint32_t)std::ceil((float)P.ef1min + slope1 * (float)sub.count)
+                        : (uint32_t)std::ceil((float)P.ef3min + slope3 * (float)sub.count);
+        b.dists = false;
+        if (form == 1) {
+          // the window (l, r) and the slab's positions inside the category (:275-282)
+          b.hb.resize((size_t)m * 2);
+          b.hib.resize((size_t)m * 2);
+          for (uint32_t j = 0; j < m; ++j) {
+            const float *mt = metas + (size_t)list[j] * 4;
+            b.hb[2 * j] = mt[2];
+            b.hb[2 * j + 1] = mt[3];
+            b.hib[2 * j] = (int32_t)(h_desc[list[j]].s - sub.start);
+            b.hib[2 * j + 1] = (int32_t)(h_desc[list[j]].e - sub.start);
+          }
         }
-        rc = launch_graph(r, sub, FKNN_GRAPH_CATEGORY_RANGE, r->qsub.p, m, Kp, R, hb.data(), hib.data(), r->lids.p,
-                          nullptr);
+        S.n_category += m;
+        B.push_back(std::move(b));
       }
-      if (rc) return rc;
-      ++S.n_graph_calls;
-      S.n_category += m;
-      k_local_to_ids<<<grid_of((uint64_t)m * R), 256, 0, st>>>(r->lids.p, (uint64_t)m * R, sub.start, r->d_cat_ids,
-                                                               r->cand.p);
-      g_launches += 1;
-      if ((rc = rerank_rows(list, R))) return rc;
+    }
+    if ((rc = run_stage(B, none, false))) return rc;
+    std::vector<uint32_t> all;
+    for (GBatch &b : B) all.insert(all.end(), b.list->begin(), b.list->end());
+    if (!all.empty()) {
+      if ((rc = r->cand.get(all.size() * R))) return rc;
+      for (GBatch &b : B) {
+        const uint64_t tot = (uint64_t)b.list->size() * R;
+        k_local_to_ids<<<grid_of(tot), 256, 0, st>>>(r->lids.p + b.o0, tot, subs(b.sub).start, r->d_cat_ids,
+                                                     r->cand.p + b.o0);
+        g_launches += 1;
+      }
+      if ((rc = rerank_rows(all, R))) return rc;
     }
   }
-
   S.ms_category = lap();
 
   // 3. types 0 and 2: candidates of several time buckets merged per query
   //    into a pool of graph_refine_k (maxPQIFCS<int>), then FP32 re-rank
   std::vector<fknn::IntPool> pool(nq);
-  std::vector<int32_t> h_ids;
-  std::vector<float> h_d;
-  // one batched graph search of `list` on bucket b; candidates offered to
-  // the pools in the searcher's slot order (ids in timestamp order)
-  auto bucket_search = [&](const fknn_router::Sub &b, int mode, const std::vector<uint32_t> &list, uint32_t Kp,
-                           const std::vector<float> *hb, const std::vector<int32_t> *hib) -> int {
-    const uint32_t m = (uint32_t)list.size();
-    if (!m) return FKNN_OK;
-    int rc2;
-    if ((rc2 = gather_queries(list)) || (rc2 = r->lids.get((size_t)m * R)) || (rc2 = r->ldist.get((size_t)m * R)))
-      return rc2;
-    if ((rc2 = launch_graph(r, b, mode, r->qsub.p, m, Kp, R, hb ? hb->data() : nullptr, hib ? hib->data() : nullptr,
-                            r->lids.p, r->ldist.p)))
-      return rc2;
-    ++S.n_graph_calls;
-    h_ids.resize((size_t)m * R);
-    h_d.resize((size_t)m * R);
-    FKNN_CUDA(cudaMemcpyAsync(h_ids.data(), r->lids.p, (size_t)m * R * 4, cudaMemcpyDeviceToHost, st));
-    FKNN_CUDA(cudaMemcpyAsync(h_d.data(), r->ldist.p, (size_t)m * R * 4, cudaMemcpyDeviceToHost, st));
-    FKNN_CUDA(cudaStreamSynchronize(st));
-    for (uint32_t j = 0; j < m; ++j) {
-      fknn::IntPool &pl = pool[list[j]];
-      if (pl.cap == 0) pl.reset((int)R);
-      for (uint32_t t = 0; t < R; ++t) pl.offer(h_ids[(size_t)j * R + t] + (int)b.start, (int)h_d[(size_t)j * R + t]);
-    }
-    return FKNN_OK;
-  };
-  // type 0: SearchFilterSubTime with ef0_full on every bucket (:303-333)
-  for (const fknn_router::Sub &b : r->bks)
-    if ((rc = bucket_search(b, FKNN_GRAPH_FILTER_SUBTIME, type0, P.ef0_full, nullptr, nullptr))) return rc;
-  S.ms_type0 = lap();
-
-  // type 2: SplitInterval (:91-134) with bf_thr 0.5 when sel < 0.2, else 0.2
-  if (!type2.empty()) {
+  {
+    const uint32_t nc = (uint32_t)r->cats.size();
+    std::vector<GBatch> B;
+    std::vector<BBatch> BB;
+    std::deque<std::vector<uint32_t>> lists;  // FULL / MEDIUM lists (stable addresses)
+    // type 0 (:303-333): SearchFilterSubTime with ef0_full on every bucket, in the map's order
+    if (!type0.empty())
+      for (uint32_t bi = 0; bi < r->bks.size(); ++bi) {
+        GBatch b;
+        b.sub = nc + bi;
+        b.mode = FKNN_GRAPH_FILTER_SUBTIME;
+        b.list = &type0;
+        b.K = P.ef0_full;
+        b.dists = true;
+        B.push_back(std::move(b));
+      }
+    const size_t n0 = B.size();
+    // type 2: SplitInterval (:91-134) with bf_thr 0.5 when sel < 0.2, else 0.2,
+    // buckets in t order (:378); per bucket its batches, then its SMALL brute force
     std::vector<size_t> border(r->bks.size());
     for (size_t b = 0; b < border.size(); ++b) border[b] = b;
     std::sort(border.begin(), border.end(), [&](size_t a, size_t c) { return r->bks[a].key < r->bks[c].key; });
-    for (size_t bi : border) {  // buckets in t order (:378)
-      const fknn_router::Sub &b = r->bks[bi];
-      const float tsb = (float)b.key / 10, teb = (float)(b.key + 1) / 10;
-      const float *tb = r->ts_full.data() + b.start;
-      // per query: FULL / MEDIUM / SMALL with its pool size
-      std::vector<uint32_t> fl[3], md[3], sm_list;
-      std::vector<uint32_t> sm_s, sm_n;
-      std::vector<float> mdb[3];
-      std::vector<int32_t> mdib[3];
-      for (uint32_t i : type2) {
-        const float l = metas[(size_t)i * 4 + 2], rr = metas[(size_t)i * 4 + 3], s = sel[i];
-        if (rr < tsb || l > teb) continue;
-        if (l <= tsb && rr >= teb) {
-          const int ki = s < 0.3f ? 0 : s < 0.6f ? 1 : 2;
-          fl[ki].push_back(i);
-          continue;
-        }
-        const float lb = std::max(tsb, l), rb = std::min(teb, rr);
-        const uint32_t s0 = (uint32_t)(std::lower_bound(tb, tb + b.count, lb) - tb);
-        const uint32_t e0 = (uint32_t)(std::upper_bound(tb, tb + b.count, rb) - tb);
-        const uint32_t np = e0 > s0 ? e0 - s0 : 0;
-        const float lsel = (float)np / (float)b.count;
-        const float thr = s < 0.2f ? 0.5f : 0.2f;
-        if (lsel < thr) {
-          if (np) {
-            sm_list.push_back(i);
-            sm_s.push_back(s0);
-            sm_n.push_back(np);
+    std::vector<size_t> bk_b0, bk_b1, bk_bb;  // per bucket (t order): its range of B, its BB index (or SIZE_MAX)
+    if (!type2.empty())
+      for (size_t bi : border) {
+        const fknn_router::Sub &b = r->bks[bi];
+        const float tsb = (float)b.key / 10, teb = (float)(b.key + 1) / 10;
+        const float *tb = r->ts_full.data() + b.start;
+        std::vector<uint32_t> fl[3], md[3];
+        std::vector<float> mdb[3];
+        std::vector<int32_t> mdib[3];
+        BBatch small;
+        small.sub = nc + (uint32_t)bi;
+        for (uint32_t i : type2) {
+          const float l = metas[(size_t)i * 4 + 2], rr = metas[(size_t)i * 4 + 3], s = sel[i];
+          if (rr < tsb || l > teb) continue;
+          if (l <= tsb && rr >= teb) {
+            fl[s < 0.3f ? 0 : s < 0.6f ? 1 : 2].push_back(i);
+            continue;
           }
-        } else {
-          const int ki = s > 0.6f ? 0 : s > 0.3f ? 1 : 2;
-          md[ki].push_back(i);
-          mdb[ki].push_back(l);
-          mdb[ki].push_back(rr);
-          mdib[ki].push_back((int32_t)s0);
-          mdib[ki].push_back((int32_t)(s0 + np - 1));
-        }
-      }
-      // the reference visits a bucket's queries in query order, each with
-      // its own form; forms are batched here, and a query meets a bucket
-      // once, so its pool sees the same sequence of candidates
-      const uint32_t kfull[3] = {P.ef2_full_small, P.ef2_full_medium, P.ef2_full_large};
-      const uint32_t kmed[3] = {P.ef2_medium_large, P.ef2_medium_medium, P.ef2_medium_small};
-      for (int ki = 0; ki < 3; ++ki) {
-        S.n_split_full += (uint32_t)fl[ki].size();
-        S.n_split_medium += (uint32_t)md[ki].size();
-        if ((rc = bucket_search(b, FKNN_GRAPH_FILTER_SUBTIME, fl[ki], kfull[ki], nullptr, nullptr))) return rc;
-        if ((rc = bucket_search(b, FKNN_GRAPH_RANGE_SUBTIME, md[ki], kmed[ki], &mdb[ki], &mdib[ki]))) return rc;
-      }
-      if (!sm_list.empty()) {
-        // SQ8 brute force over the bucket's own codes (its searcher's
-        // quantizer), distances times alpha^2 (:399-417, bruteforce.h:267)
-        const uint32_t m = (uint32_t)sm_list.size(), kb = P.bf_refine_k;
-        S.n_split_small += m;
-        const int8_t *bcodes;
-        float ba;
-        uint32_t bn;
-        graph_codes(b.g, &bcodes, &ba, &bn);
-        std::vector<uint32_t> h_sel((size_t)m * 3);
-        for (uint32_t j = 0; j < m; ++j) {
-          h_sel[3 * j] = j;
-          h_sel[3 * j + 1] = sm_s[j];
-          h_sel[3 * j + 2] = sm_s[j] + sm_n[j];
-        }
-        if ((rc = gather_queries(sm_list)) || (rc = r->qcodes_b.get((size_t)m * CODE)) ||
-            (rc = r->sel.get((size_t)m * 3)) || (rc = r->keys.get((size_t)m * kb)))
-          return rc;
-        launch_sq8_encode(r->qsub.p, m, ba, r->qcodes_b.p, st);
-        FKNN_CUDA(cudaMemcpyAsync(r->sel.p, h_sel.data(), (size_t)m * 12, cudaMemcpyHostToDevice, st));
-        k_sq8_slab_topk<<<std::min<uint32_t>(m, 148 * 8), ST_THREADS, 0, st>>>(bcodes, bcodes, r->qcodes_b.p, r->sel.p,
-                                                                              nullptr, m, kb, r->keys.p);
-        g_launches += 2;
-        std::vector<uint64_t> hk((size_t)m * kb);
-        FKNN_CUDA(cudaMemcpyAsync(hk.data(), r->keys.p, hk.size() * 8, cudaMemcpyDeviceToHost, st));
-        FKNN_CUDA(cudaStreamSynchronize(st));
-        const float a2 = ba * ba;
-        for (uint32_t j = 0; j < m; ++j) {
-          fknn::IntPool &pl = pool[sm_list[j]];
-          if (pl.cap == 0) pl.reset((int)R);
-          for (uint32_t t = 0; t < kb; ++t) {
-            const uint64_t key = hk[(size_t)j * kb + t];
-            if (key == ~0ull) break;
-            const float dist = (float)(uint32_t)(key >> 32) * ba * ba;
-            (void)a2;
-            pl.offer((int)(b.start + sm_s[j] + (uint32_t)key), (int)dist);
+          const float lb = std::max(tsb, l), rb = std::min(teb, rr);
+          const uint32_t s0 = (uint32_t)(std::lower_bound(tb, tb + b.count, lb) - tb);
+          const uint32_t e0 = (uint32_t)(std::upper_bound(tb, tb + b.count, rb) - tb);
+          const uint32_t np_ = e0 > s0 ? e0 - s0 : 0;
+          const float lsel = (float)np_ / (float)b.count;
+          const float thr = s < 0.2f ? 0.5f : 0.2f;
+          if (lsel < thr) {
+            if (np_) {
+              small.list.push_back(i);
+              small.s.push_back(s0);
+              small.cnt.push_back(np_);
+            }
+          } else {
+            const int ki = s > 0.6f ? 0 : s > 0.3f ? 1 : 2;
+            md[ki].push_back(i);
+            mdb[ki].push_back(l);
+            mdb[ki].push_back(rr);
+            mdib[ki].push_back((int32_t)s0);
+            mdib[ki].push_back((int32_t)(s0 + np_ - 1));
           }
+        }
+        const uint32_t kfull[3] = {P.ef2_full_small, P.ef2_full_medium, P.ef2_full_large};
+        const uint32_t kmed[3] = {P.ef2_medium_large, P.ef2_medium_medium, P.ef2_medium_small};
+        bk_b0.push_back(B.size());
+        for (int ki = 0; ki < 3; ++ki) {
+          S.n_split_full += (uint32_t)fl[ki].size();
+          S.n_split_medium += (uint32_t)md[ki].size();
+          if (!fl[ki].empty()) {
+            lists.push_back(std::move(fl[ki]));
+            GBatch g;
+            g.sub = nc + (uint32_t)bi;
+            g.mode = FKNN_GRAPH_FILTER_SUBTIME;
+            g.list = &lists.back();
+            g.K = kfull[ki];
+            g.dists = true;
+            B.push_back(std::move(g));
+          }
+          if (!md[ki].empty()) {
+            lists.push_back(std::move(md[ki]));
+            GBatch g;
+            g.sub = nc + (uint32_t)bi;
+            g.mode = FKNN_GRAPH_RANGE_SUBTIME;
+            g.list = &lists.back();
+            g.K = kmed[ki];
+            g.hb = std::move(mdb[ki]);
+            g.hib = std::move(mdib[ki]);
+            g.dists = true;
+            B.push_back(std::move(g));
+          }
+        }
+        bk_b1.push_back(B.size());
+        S.n_split_small += (uint32_t)small.list.size();
+        bk_bb.push_back(small.list.empty() ? SIZE_MAX : BB.size());
+        if (!small.list.empty()) BB.push_back(std::move(small));
+      }
+    if ((rc = run_stage(B, BB, true))) return rc;
+    S.ms_type0 = lap();
+    // the pools, in the reference's order of offers (a query meets a bucket once)
+    auto offer_graph = [&](const GBatch &b) {
+      const fknn_router::Sub &sub = subs(b.sub);
+      for (size_t j = 0; j < b.list->size(); ++j) {
+        fknn::IntPool &pl = pool[(*b.list)[j]];
+        if (pl.cap == 0) pl.reset((int)R);
+        const size_t o = b.o0 + j * R;
+        for (uint32_t t = 0; t < R; ++t) pl.offer(h_ids[o + t] + (int)sub.start, (int)h_d[o + t]);
+      }
+    };
+    for (size_t i = 0; i < n0; ++i) offer_graph(B[i]);
+    const uint32_t kb = P.bf_refine_k;
+    for (size_t k = 0; k < bk_b0.size(); ++k) {
+      for (size_t i = bk_b0[k]; i < bk_b1[k]; ++i) offer_graph(B[i]);
+      if (bk_bb[k] == SIZE_MAX) continue;
+      // SQ8 distances over the bucket's own codes times alpha^2 (:399-417, bruteforce.h:267)
+      const BBatch &b = BB[bk_bb[k]];
+      const fknn_router::Sub &sub = subs(b.sub);
+      const int8_t *bcodes;
+      float ba;
+      uint32_t bn;
+      graph_codes(sub.g, &bcodes, &ba, &bn);
+      for (size_t j = 0; j < b.list.size(); ++j) {
+        fknn::IntPool &pl = pool[b.list[j]];
+        if (pl.cap == 0) pl.reset((int)R);
+        for (uint32_t t = 0; t < kb; ++t) {
+          const uint64_t key = h_keys[b.k0 + j * kb + t];
+          if (key == ~0ull) break;
+          const float dist = (float)(uint32_t)(key >> 32) * ba * ba;
+          pl.offer((int)(sub.start + b.s[j] + (uint32_t)key), (int)dist);
         }
       }
     }
