@@ -39,17 +39,13 @@ namespace {
 
 constexpr int FC_THREADS = 512;
 constexpr int FC_WARPS = FC_THREADS / 32;
-constexpr int FC_SEG = 128;                        // rows per segment: one set of four ballot words
-constexpr int FC_SEGS = 2;                         // segments per warp in a tile
-constexpr int FC_TSEG = FC_WARPS * FC_SEGS;        // segments per tile (32)
-constexpr int FC_TILE = FC_TSEG * FC_SEG;          // rows per tile (4,096)
-constexpr uint32_t FP_MAXP = 16;                   // predicates per launch
-constexpr uint32_t FC_STAGE_BYTES = 2 * FC_TILE * 4;  // one ring stage: a tile of both columns (32 KB)
-constexpr uint32_t FC_SMAX = 3;                    // ring stages at most
-constexpr uint32_t FC_LAG = 2;                     // rows between a tile's count and its ids
-constexpr uint32_t FC_SLOTS = FC_LAG + 2;          // bits slots (the writer's, the counter's and one between)
-constexpr size_t FC_SMEM_MAX = 108 * 1024;         // dynamic shared memory per CTA: two CTAs share an SM
-constexpr int FC_SUM_UNROLL = 10;                  // tile counts per lane of a row (rows of up to 320 CTAs)
+constexpr int FC_STEP = FC_THREADS * 4;  // rows per CTA step: a float4 of each column per thread
+constexpr int FC_SEG = 128;              // rows per warp segment
+constexpr uint32_t FP_MAXP = 16;         // predicates per launch
+constexpr size_t FC_SMEM_MAX = 104 * 1024;  // ring + bits + offsets per CTA, so that two CTAs share an SM
+constexpr uint32_t FC_STAGE_BYTES = 2 * FC_STEP * 4;  // one ring stage: FC_STEP rows of both columns
+constexpr uint32_t FC_SMAX = 6;                      // ring stages at most
+constexpr int FC_SUM_UNROLL = 10;           // CTA totals in flight per lane (one pass for up to 320 CTAs)
 
 static_assert(FC_WARPS >= (int)FP_MAXP, "one warp per predicate sums the CTA totals");
 
@@ -93,215 +89,243 @@ __device__ __forceinline__ void load_step(const float *__restrict__ labels, cons
   }
 }
 
-// Grid: G CTAs, all resident (cooperative launch).  Tiles of FC_TILE rows in
-// row order; CTA c takes tiles j * G + c, j = 0 .. nrow - 1 ("row" j of
-// tiles).  At step j a CTA counts its tile of row j (bits and counts kept
-// in a shared-memory slot, its tile count published), and writes the ids of
-// its tile of row j - FC_LAG, whose place is the counts of all tiles before
-// it: the rows before (a running total) plus the CTAs before it in its row.
-// Those counts were published FC_LAG steps earlier, so the ids stream out
-// while the columns stream in.  Dynamic shared memory: S ring stages of
-// FC_TILE rows of both columns (bulk copies), FC_SLOTS slots of np x
-// FC_TSEG bits and segment offsets, a 128-id staging slice per warp.
-// agg: nrow x G x FP_MAXP words (epoch tag << 16 | tile count); flag: the
-// failure flag (tagged with ep).  Row ids fit 32 bits (n < 2^31).
+// Grid: G CTAs, all resident.  Rows per CTA per round: R (a multiple of
+// FC_STEP).  Dynamic shared memory: S ring stages of FC_STEP rows of both
+// columns (bulk copies), then np x nseg x uint4 bits and np x nseg segment
+// offsets (nseg = R / FC_SEG).  sync: [0] the arrival counter (value
+// bar_base at this launch), [1] the failure flag, [2 ..] 2 x G x FP_MAXP
+// per-round CTA totals (double-buffered by round parity).  Row ids fit
+// 32 bits (n < 2^31).
 __global__ void __launch_bounds__(FC_THREADS, 2)
     k_filter_coop(const float *__restrict__ labels, const float *__restrict__ ts, uint32_t n, FilterPreds P,
-                  uint32_t np, uint32_t nrow, uint32_t S, uint32_t *agg, uint64_t *flag, uint32_t ep,
-                  uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts, int *err) {
+                  uint32_t np, uint32_t R, uint32_t rounds, uint32_t S, uint64_t *sync, uint64_t bar_base,
+                  uint32_t ep, uint32_t *__restrict__ out, uint64_t out_stride, uint64_t *__restrict__ counts,
+                  int *err) {
   extern __shared__ __align__(128) unsigned char fc_smem[];
-  float *ring = reinterpret_cast<float *>(fc_smem);  // stage st: labels [FC_TILE], ts [FC_TILE]
-  uint4 *bits = reinterpret_cast<uint4 *>(fc_smem + (size_t)S * FC_STAGE_BYTES);   // [slot][np][FC_TSEG]
-  uint32_t *segx = reinterpret_cast<uint32_t *>(bits + (size_t)FC_SLOTS * np * FC_TSEG);  // same shape
-  uint32_t *stage_all = segx + (size_t)FC_SLOTS * np * FC_TSEG;                     // [warp][FC_SEG]
+  const uint32_t nseg = R / FC_SEG, nchunk = R / FC_STEP;
+  float *ring = reinterpret_cast<float *>(fc_smem);  // stage st: labels [FC_STEP], ts [FC_STEP]
+  uint4 *bits = reinterpret_cast<uint4 *>(fc_smem + (size_t)S * FC_STAGE_BYTES);  // [np][nseg]
+  uint32_t *segoff = reinterpret_cast<uint32_t *>(bits + (size_t)np * nseg);      // [np][nseg]
   __shared__ uint64_t full[FC_SMAX];
   __shared__ float4 pb[FP_MAXP];
-  __shared__ uint32_t s_pref[FP_MAXP];
-  __shared__ uint64_t s_rowbase[FP_MAXP];
+  __shared__ uint32_t wtot[FP_MAXP][FC_WARPS], wsum[FP_MAXP][FC_WARPS];
+  __shared__ uint64_t s_off[FP_MAXP], s_base[FP_MAXP];
+  __shared__ int s_fail;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5;
   const uint32_t G = gridDim.x, cta = blockIdx.x;
-  const uint32_t tag = (ep & 0xffffu) << 16;
   if (tid < (int)FP_MAXP) {
     pb[tid] = P.b[tid];
-    s_rowbase[tid] = 0;
+    s_base[tid] = 0;
   }
   if (tid == 0) {
     for (uint32_t st = 0; st < S; ++st) mbar_init(&full[st], 1);
     fence_mbar_init();
   }
   __syncthreads();
+  unsigned long long *bar = reinterpret_cast<unsigned long long *>(sync);
+  uint64_t *flag = sync + 1, *part = sync + 2;
   const uint32_t lanemask_lt = (1u << lane) - 1u;
-  auto tile_full = [&](uint32_t t) { return (uint64_t)(t + 1) * FC_TILE <= n; };
-  auto issue = [&](uint32_t t, uint32_t st) {
-    float *dst = ring + st * (2 * FC_TILE);
-    mbar_arrive_expect_tx(&full[st], FC_STAGE_BYTES);
-    bulk_g2s(dst, labels + (size_t)t * FC_TILE, FC_TILE * 4, &full[st]);
-    bulk_g2s(dst + FC_TILE, ts + (size_t)t * FC_TILE, FC_TILE * 4, &full[st]);
-  };
-  uint32_t pend = 0;  // bit st: a copy into stage st is in flight (the same in every thread)
-  for (uint32_t j = 0; j < S && j < nrow; ++j)
-    if (tile_full(j * G + cta)) {
-      if (tid == 0) issue(j * G + cta, j);
-      pend |= 1u << j;
-    }
-  uint32_t phase = 0;         // bit st: the parity of stage st's next completion (the same in every thread)
-  uint32_t st = 0;            // ring stage of row j (j mod S)
-  uint32_t slot = 0;          // bits slot of row j (j mod FC_SLOTS)
-  uint32_t *stage = stage_all + w * FC_SEG;
-  bool failed = false;
-  for (uint32_t j = 0; j < nrow + FC_LAG; ++j) {
-    const bool counting = j < nrow, writing = j >= FC_LAG;
-    const uint32_t jw = j - FC_LAG, wslot = (slot + FC_SLOTS - FC_LAG) % FC_SLOTS;
-    // the counts of row jw, loaded early (published FC_LAG steps ago)
-    uint32_t x[FC_SUM_UNROLL];
-    if (writing && w < (int)np) {
-#pragma unroll
-      for (int k = 0; k < FC_SUM_UNROLL; ++k) {
-        const uint32_t c2 = k * 32 + lane;
-        x[k] = c2 < G ? ld_volatile_u32(agg + ((size_t)jw * G + c2) * FP_MAXP + w) : tag;
-      }
-    }
-    // ---- count the tile of row j
-    if (counting) {
-      const uint32_t t = j * G + cta;
-      float4 la[FC_SEGS], tb[FC_SEGS];
-      uint32_t vb[FC_SEGS];
-      if (tile_full(t)) {
+  uint32_t phase = 0;  // bit st: the parity of stage st's next completion (the same in every thread)
+
+  for (uint32_t rd = 0; rd < rounds; ++rd) {
+    const uint32_t cbase = (rd * G + cta) * R;  // the CTA's first row this round
+    // chunks 0 .. nfull-1 have all their rows and are copied in bulk; the
+    // (one) partial chunk of the base is read by the threads themselves
+    const uint32_t nfull = n > cbase ? min(nchunk, (n - cbase) / FC_STEP) : 0u;
+    auto issue = [&](uint32_t c, uint32_t st) {
+      float *dst = ring + st * (2 * FC_STEP);
+      mbar_arrive_expect_tx(&full[st], FC_STAGE_BYTES);
+      bulk_g2s(dst, labels + cbase + c * FC_STEP, FC_STEP * 4, &full[st]);
+      bulk_g2s(dst + FC_STEP, ts + cbase + c * FC_STEP, FC_STEP * 4, &full[st]);
+    };
+    if (tid == 0)
+      for (uint32_t c = 0; c < S && c < nfull; ++c) issue(c, c);
+    for (uint32_t p = tid; p < np * FC_WARPS; p += FC_THREADS) wsum[p / FC_WARPS][p % FC_WARPS] = 0;
+    __syncthreads();
+    // ---- 1. pass bits per warp segment (segment c * FC_WARPS + w: rows
+    //         cbase + c * FC_STEP + w * FC_SEG + 4 * lane + 0..3)
+    bool gave_up = false;
+    uint32_t c = 0, st = 0;  // chunk, its ring stage (c mod S)
+    const float *mine = ring + w * FC_SEG + 4 * lane;
+    for (; c < nchunk; ++c) {
+      const uint32_t seg = c * FC_WARPS + w;
+      float4 la, tb;
+      uint32_t vb = 0xfu;
+      if (c < nfull) {
         // warp-uniform: the lanes' timers may disagree at the deadline
-        if (__all_sync(0xffffffffu, mbar_wait_bounded(&full[st], (phase >> st) & 1u, err))) {
-          phase ^= 1u << st;
-          pend &= ~(1u << st);
-        } else {
-          failed = true;  // the copy is still pending, at the same parity
-        }
-        const float *src = ring + st * (2 * FC_TILE) + w * (FC_SEGS * FC_SEG) + 4 * lane;
-#pragma unroll
-        for (int sg = 0; sg < FC_SEGS; ++sg) {
-          la[sg] = *reinterpret_cast<const float4 *>(src + sg * FC_SEG);
-          tb[sg] = *reinterpret_cast<const float4 *>(src + sg * FC_SEG + FC_TILE);
-          vb[sg] = 0xfu;
-        }
+        if (!__all_sync(0xffffffffu, mbar_wait_bounded(&full[st], (phase >> st) & 1u, err))) gave_up = true;
+        phase ^= 1u << st;
+        la = *reinterpret_cast<const float4 *>(mine + st * (2 * FC_STEP));
+        tb = *reinterpret_cast<const float4 *>(mine + st * (2 * FC_STEP) + FC_STEP);
       } else {
-#pragma unroll
-        for (int sg = 0; sg < FC_SEGS; ++sg)
-          load_step(labels, ts, n, t * FC_TILE + w * (FC_SEGS * FC_SEG) + sg * FC_SEG + 4 * lane, la[sg], tb[sg],
-                    vb[sg]);
+        load_step(labels, ts, n, cbase + c * FC_STEP + w * FC_SEG + 4 * lane, la, tb, vb);
       }
       for (uint32_t p = 0; p < np; ++p) {
+        const uint32_t b4 = pred_bits4(pb[p], la, tb) & vb;
+        const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
+        const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
+        if (lane == 0) {
+          const uint32_t cnt = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+          bits[p * nseg + seg] = make_uint4(m0, m1, m2, m3);
+          segoff[p * nseg + seg] = cnt;
+          wsum[p][w] += cnt;
+        }
+      }
+      // the stage is free once every warp has read it; refill it
+      if (__syncthreads_or(gave_up)) {
+        gave_up = true;
+        break;
+      }
+      if (tid == 0 && c + S < nfull) issue(c + S, st);
+      if (++st == S) st = 0;
+    }
+    if (gave_up) {
+      // a copy did not land in time: wait (bounded) for this CTA's copies
+      // still in flight, flag the launch and poison the counts
+      if (tid == 0) {
+        uint32_t st2 = st;
+        for (uint32_t c2 = c; c2 < c + S && c2 < nfull; ++c2) {
+          const uint32_t par = c2 == c ? (((phase >> st2) & 1u) ^ 1u) : ((phase >> st2) & 1u);
+          mbar_wait_bounded(&full[st2], par, err);
+          if (++st2 == S) st2 = 0;
+        }
+        *(volatile uint64_t *)flag = ep;
+        __threadfence();
+      }
+      __syncthreads();
+      if (tid < (int)np) counts[tid] = ~0ull;
+      return;
+    }
+    // ---- 2. the CTA's totals, published; the barrier arrival (release)
+    if (tid == 0) {
+      uint64_t *mypart = part + ((size_t)(rd & 1) * G + cta) * FP_MAXP;
+      for (uint32_t p = 0; p < np; ++p) {
+        uint32_t t = 0;
+        for (int j = 0; j < FC_WARPS; ++j) t += wsum[p][j];
+        mypart[p] = t;
+      }
+      asm volatile("red.release.gpu.global.add.u64 [%0], %1;" ::"l"(bar), "l"(1ull) : "memory");
+    }
+    // ---- 3. segment offsets inside the CTA, while the other CTAs finish
+    for (uint32_t i0 = 0; i0 < nseg; i0 += FC_THREADS) {
+      const uint32_t i = i0 + tid;
+      for (uint32_t p = 0; p < np; ++p) {
+        const uint32_t v = i < nseg ? segoff[p * nseg + i] : 0u;
+        uint32_t inc = v;
 #pragma unroll
-        for (int sg = 0; sg < FC_SEGS; ++sg) {
-          const uint32_t b4 = pred_bits4(pb[p], la[sg], tb[sg]) & vb[sg];
-          const uint32_t m0 = __ballot_sync(0xffffffffu, b4 & 1u), m1 = __ballot_sync(0xffffffffu, b4 & 2u);
-          const uint32_t m2 = __ballot_sync(0xffffffffu, b4 & 4u), m3 = __ballot_sync(0xffffffffu, b4 & 8u);
-          if (lane == 0) {
-            const uint32_t i = (slot * np + p) * FC_TSEG + w * FC_SEGS + sg;
-            bits[i] = make_uint4(m0, m1, m2, m3);
-            segx[i] = __popc(m0) + __popc(m1) + __popc(m2) + __popc(m3);
+        for (int o = 1; o < 32; o <<= 1) {
+          const uint32_t x = __shfl_up_sync(0xffffffffu, inc, o);
+          if (lane >= o) inc += x;
+        }
+        if (i < nseg) segoff[p * nseg + i] = inc - v;  // exclusive within the warp's 32 segments
+        if (lane == 31) wtot[p][w] = inc;
+      }
+      __syncthreads();
+      if (tid < (int)np) {  // the warps' totals -> exclusive prefixes, carried across chunks of segments
+        uint32_t acc = i0 ? (uint32_t)s_off[tid] : 0u;  // the running total of the earlier chunks
+        for (int j = 0; j < FC_WARPS; ++j) {
+          const uint32_t x = wtot[tid][j];
+          wtot[tid][j] = acc;
+          acc += x;
+        }
+        s_off[tid] = acc;
+      }
+      __syncthreads();
+      if (i < nseg)
+        for (uint32_t p = 0; p < np; ++p) segoff[p * nseg + i] += wtot[p][w];
+      __syncthreads();
+    }
+    // ---- 4. the grid barrier's wait (bounded, acquire)
+    if (tid == 0) {
+      const uint64_t target = bar_base + (uint64_t)(rd + 1) * G;
+      auto now = [&]() {
+        uint64_t v;
+        asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(bar) : "memory");
+        return v;
+      };
+      int f = 0;
+      if (now() < target) {
+        const uint64_t t0 = global_ns();
+        while (now() < target) {
+          if (global_ns() - t0 > WAIT_NS) {
+            f = 1;
+            break;
           }
         }
       }
+      s_fail = f;
     }
-    if (__syncthreads_or(failed)) {
-      failed = true;
-      break;
-    }
-    if (counting) {
-      if (tid < (int)np) {
-        // segment offsets inside the tile; the tile's count, published
-        uint32_t *sx = segx + (slot * np + tid) * FC_TSEG, acc = 0;
-        for (int i = 0; i < FC_TSEG; ++i) {
-          const uint32_t v = sx[i];
-          sx[i] = acc;
-          acc += v;
-        }
-        *(volatile uint32_t *)(agg + ((size_t)j * G + cta) * FP_MAXP + tid) = tag | acc;
+    __syncthreads();
+    if (s_fail) {
+      if (tid == 0) {
+        *(volatile uint64_t *)flag = ep;
+        __threadfence();
       }
-      // the stage of row j is free (every warp is past the barrier): refill it
-      if (j + S < nrow && tile_full((j + S) * G + cta)) {
-        if (tid == 0) issue((j + S) * G + cta, st);
-        pend |= 1u << st;
-      }
-      if (++st == S) st = 0;
+      __syncthreads();
+      if (tid < (int)np) counts[tid] = ~0ull;
+      return;
     }
-    // ---- the place of this CTA's tile of row jw
-    if (writing && w < (int)np) {
-      const uint64_t t0 = global_ns();
-      bool ok = true;
+    // ---- the CTAs before this one: this CTA's offset; all: the round total
+    if (w < (int)np) {
+      const uint64_t *rp = part + (size_t)(rd & 1) * G * FP_MAXP;
+      uint64_t before = 0, all = 0;
+      for (uint32_t c0 = 0; c0 < G; c0 += 32 * FC_SUM_UNROLL) {
+        uint64_t x[FC_SUM_UNROLL];
 #pragma unroll
-      for (int k = 0; k < FC_SUM_UNROLL; ++k) {
-        const uint32_t c2 = k * 32 + lane;
-        while (ok && (x[k] & 0xffff0000u) != tag) {
-          if (global_ns() - t0 > WAIT_NS) ok = false;
-          else x[k] = ld_volatile_u32(agg + ((size_t)jw * G + c2) * FP_MAXP + w);
+        for (int j = 0; j < FC_SUM_UNROLL; ++j) {  // the loads first, all in flight
+          const uint32_t cc = c0 + j * 32 + lane;
+          x[j] = cc < G ? __ldcg(rp + (size_t)cc * FP_MAXP + w) : 0ull;
         }
-      }
-      uint32_t before = 0, all = 0;
 #pragma unroll
-      for (int k = 0; k < FC_SUM_UNROLL; ++k) {
-        const uint32_t c2 = k * 32 + lane, v = c2 < G ? (x[k] & 0xffffu) : 0u;
-        all += v;
-        if (c2 < cta) before += v;
+        for (int j = 0; j < FC_SUM_UNROLL; ++j) {
+          all += x[j];
+          if (c0 + j * 32 + lane < cta) before += x[j];
+        }
       }
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) {
         before += __shfl_xor_sync(0xffffffffu, before, o);
         all += __shfl_xor_sync(0xffffffffu, all, o);
       }
-      if (!__all_sync(0xffffffffu, ok)) failed = true;
       if (lane == 0) {
-        s_pref[w] = (uint32_t)s_rowbase[w] + before;
-        s_rowbase[w] += all;
+        s_off[w] = s_base[w] + before;
+        s_base[w] += all;
       }
-    }
-    if (__syncthreads_or(failed)) {
-      failed = true;
-      break;
-    }
-    // ---- its ids, staged per segment and stored contiguously
-    if (writing) {
-      const uint32_t tw = jw * G + cta;
-      for (uint32_t p = 0; p < np; ++p) {
-        uint32_t *op = out + p * out_stride;
-#pragma unroll
-        for (int sg = 0; sg < FC_SEGS; ++sg) {
-          const uint32_t i = (wslot * np + p) * FC_TSEG + w * FC_SEGS + sg;
-          const uint4 m = bits[i];  // the same for the whole warp: the skip is uniform
-          const uint32_t cnt = __popc(m.x) + __popc(m.y) + __popc(m.z) + __popc(m.w);
-          if (cnt == 0) continue;
-          const uint32_t b4 = ((m.x >> lane) & 1u) | (((m.y >> lane) & 1u) << 1) | (((m.z >> lane) & 1u) << 2) |
-                              (((m.w >> lane) & 1u) << 3);
-          uint32_t k = __popc(m.x & lanemask_lt) + __popc(m.y & lanemask_lt) + __popc(m.z & lanemask_lt) +
-                       __popc(m.w & lanemask_lt);
-          const uint32_t r = tw * FC_TILE + w * (FC_SEGS * FC_SEG) + sg * FC_SEG + 4 * lane;
-#pragma unroll
-          for (int q = 0; q < 4; ++q)
-            if ((b4 >> q) & 1u) stage[k++] = r + q;
-          __syncwarp();
-          uint32_t *dst = op + s_pref[p] + segx[i];
-          for (uint32_t jj = lane; jj < cnt; jj += 32) dst[jj] = stage[jj];
-          __syncwarp();  // the slice is rewritten by the next segment
-        }
-      }
-    }
-    if (++slot == FC_SLOTS) slot = 0;
-  }
-  if (failed) {
-    // a wait gave up: wait (bounded) for this CTA's copies still in flight,
-    // flag the launch and poison the counts
-    if (tid == 0) {
-      for (uint32_t s2 = 0; s2 < S; ++s2)
-        if ((pend >> s2) & 1u) mbar_wait_bounded(&full[s2], (phase >> s2) & 1u, err);
-      *(volatile uint64_t *)flag = ep;
-      __threadfence();
     }
     __syncthreads();
-    if (tid < (int)np) counts[tid] = ~0ull;
-    return;
+    // ---- 5. ids of the passing rows: per segment staged in this warp's
+    //         slice of the (now idle) ring, then stored contiguously
+    uint32_t *stage = reinterpret_cast<uint32_t *>(ring) + w * FC_SEG;
+    for (uint32_t p = 0; p < np; ++p) {
+      uint32_t *op = out + p * out_stride;
+      const uint32_t base = (uint32_t)s_off[p];
+      const uint4 *bp = bits + p * nseg + w;
+      const uint32_t *sp = segoff + p * nseg + w;
+      for (uint32_t cc = 0; cc < nchunk; ++cc) {
+        const uint4 m = bp[cc * FC_WARPS];  // the same for the whole warp: the skip is uniform
+        const uint32_t cnt = __popc(m.x) + __popc(m.y) + __popc(m.z) + __popc(m.w);
+        if (cnt == 0) continue;
+        const uint32_t b4 = ((m.x >> lane) & 1u) | (((m.y >> lane) & 1u) << 1) | (((m.z >> lane) & 1u) << 2) |
+                            (((m.w >> lane) & 1u) << 3);
+        uint32_t k = __popc(m.x & lanemask_lt) + __popc(m.y & lanemask_lt) + __popc(m.z & lanemask_lt) +
+                     __popc(m.w & lanemask_lt);
+        const uint32_t r = cbase + cc * FC_STEP + w * FC_SEG + 4 * lane;
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          if ((b4 >> q) & 1u) stage[k++] = r + q;
+        __syncwarp();
+        uint32_t *dst = op + base + sp[cc * FC_WARPS];
+        for (uint32_t j = lane; j < cnt; j += 32) dst[j] = stage[j];
+        __syncwarp();  // the slice is rewritten by the next segment
+      }
+    }
+    // the ring's generic writes before the next round's bulk copies into it
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    __syncthreads();  // bits, offsets and the ring are rewritten by the next round
   }
   if (cta == 0 && tid < (int)np) {
-    __threadfence();
-    const bool bad = ld_volatile_u64(flag) == ep;
-    counts[tid] = bad ? ~0ull : s_rowbase[tid];
+    const bool failed = ld_volatile_u64(flag) == ep;
+    counts[tid] = failed ? ~0ull : s_base[tid];
   }
 }
 
@@ -384,46 +408,62 @@ int filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uint32_t
       set_error("fknn_filter_rows: the compaction kernel does not fit an SM");
       return FKNN_ECUDA;
     }
-    fs.grid = std::min<uint32_t>((uint32_t)idx->num_sms * (uint32_t)std::min(per_sm, 2), 32 * FC_SUM_UNROLL);
+    fs.grid = (uint32_t)idx->num_sms * (uint32_t)std::min(per_sm, 2);
   }
   const uint32_t G = fs.grid;
-  const uint32_t ntiles = (uint32_t)((n + FC_TILE - 1) / FC_TILE), nrow = (ntiles + G - 1) / G;
-  // the failure flag, then nrow x G x FP_MAXP tagged tile counts; cleared
-  // when the buffer is new or the 16-bit epochs run out
-  const size_t bytes = 64 + (size_t)nrow * G * FP_MAXP * 4;
-  unsigned char *sync;
+  // sync words: arrival counter, failure flag, 2 x G x FP_MAXP CTA totals;
+  // cleared when the buffer is new or the epochs run out
+  const size_t words = 2 + 2 * (size_t)G * FP_MAXP;
+  uint64_t *sync;
   int rc;
-  if ((rc = ws_get(idx, 16, bytes, (void **)&sync))) return rc;
-  if (fs.status != sync || fs.bytes != idx->ws[16].bytes || fs.epoch >= 0xffffu) {
-    FKNN_CUDA(cudaMemsetAsync(sync, 0, bytes, st));
+  if ((rc = ws_get(idx, 16, words * sizeof(uint64_t), (void **)&sync))) return rc;
+  if (fs.status != sync || fs.bytes != idx->ws[16].bytes || fs.epoch >= (1u << 30)) {
+    FKNN_CUDA(cudaMemsetAsync(sync, 0, words * sizeof(uint64_t), st));
     fs.status = sync;
     fs.bytes = idx->ws[16].bytes;
     fs.epoch = 0;
+    fs.arrivals = 0;
   }
   for (uint32_t p0 = 0; p0 < np; p0 += FP_MAXP) {
     const uint32_t m = std::min<uint32_t>(FP_MAXP, np - p0);
-    // shared memory: the bits slots, the staging slices, and as many ring
-    // stages as fit (at least one)
-    const size_t slots = (size_t)FC_SLOTS * m * FC_TSEG * (sizeof(uint4) + sizeof(uint32_t));
-    const size_t staging = (size_t)FC_WARPS * FC_SEG * sizeof(uint32_t);
-    const uint32_t S = (uint32_t)std::max<size_t>(
-        1, std::min<size_t>(FC_SMAX, (FC_SMEM_MAX - slots - staging) / FC_STAGE_BYTES));
-    const size_t smem = (size_t)S * FC_STAGE_BYTES + slots + staging;
+    // rows per CTA per round and ring stages: one round with the deepest
+    // ring the shared memory leaves room for, else two stages and as few
+    // rounds as the bits allow (rows split evenly)
+    const size_t per_seg = (size_t)m * (sizeof(uint4) + sizeof(uint32_t));  // bits + offset per 128 rows
+    const uint64_t one = ((n + G - 1) / G + FC_STEP - 1) / FC_STEP * FC_STEP;
+    uint32_t S;
+    uint64_t rounds, R;
+    if ((one / FC_SEG) * per_seg + 2 * FC_STAGE_BYTES <= FC_SMEM_MAX) {
+      rounds = 1;
+      R = one;
+      S = (uint32_t)std::min<size_t>(FC_SMAX, (FC_SMEM_MAX - (one / FC_SEG) * per_seg) / FC_STAGE_BYTES);
+    } else {
+      S = 2;
+      const uint64_t r_cap = std::max<uint64_t>(
+          FC_STEP, ((FC_SMEM_MAX - 2 * FC_STAGE_BYTES) / per_seg) * FC_SEG / FC_STEP * FC_STEP);
+      rounds = (n + G * r_cap - 1) / (G * r_cap);
+      const uint64_t per_cta = (n + G * rounds - 1) / (G * rounds);
+      R = std::max<uint64_t>(FC_STEP, (per_cta + FC_STEP - 1) / FC_STEP * FC_STEP);
+    }
+    const size_t smem = (size_t)S * FC_STAGE_BYTES + (size_t)(R / FC_SEG) * per_seg;
     FilterPreds P;
     std::memset(&P, 0, sizeof(P));
-    for (uint32_t p = 0; p < m; ++p) P.b[p] = pred_bounds(metas + (size_t)(p0 + p) * 4);
+    for (uint32_t p = 0; p < m; ++p) {
+      const float *q = metas + (size_t)(p0 + p) * 4;
+      P.b[p] = pred_bounds(q);
+    }
     const float *lab = idx->labels_f, *tsv = idx->ts_f;
-    uint32_t nn = (uint32_t)n, mm = m, nr = nrow, SS = S, ep = ++fs.epoch;
-    uint32_t *agg = reinterpret_cast<uint32_t *>(sync + 64);
-    uint64_t *flag = reinterpret_cast<uint64_t *>(sync);
-    uint64_t stride = n;
+    uint32_t nn = (uint32_t)n;
+    uint64_t bar_base = fs.arrivals, stride = n;
+    uint32_t mm = m, RR = (uint32_t)R, nr = (uint32_t)rounds, SS = S, ep = ++fs.epoch;
     uint32_t *o = d_out + (uint64_t)p0 * n;
     uint64_t *c = d_counts + p0;
     int *errp = idx->d_flag;
-    void *args[] = {(void *)&lab,  (void *)&tsv, (void *)&nn,     (void *)&P, (void *)&mm,
-                    (void *)&nr,   (void *)&SS,  (void *)&agg,    (void *)&flag, (void *)&ep,
-                    (void *)&o,    (void *)&stride, (void *)&c,   (void *)&errp};
+    void *args[] = {(void *)&lab, (void *)&tsv, (void *)&nn, (void *)&P, (void *)&mm, (void *)&RR, (void *)&nr,
+                    (void *)&SS, (void *)&sync, (void *)&bar_base, (void *)&ep, (void *)&o, (void *)&stride,
+                    (void *)&c, (void *)&errp};
     FKNN_CUDA(cudaLaunchCooperativeKernel((const void *)k_filter_coop, dim3(G), dim3(FC_THREADS), args, smem, st));
+    fs.arrivals += rounds * G;
     g_launches += 1;
   }
   FKNN_CUDA(cudaGetLastError());

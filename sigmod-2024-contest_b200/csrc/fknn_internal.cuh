@@ -222,12 +222,14 @@ struct GraphCache {
 };
 
 // The predicate compaction's persistent state over its sync buffer (ws
-// slot 16): launches tag their published tile counts and their failure
-// flag with an epoch, so no launch clears anything.
+// slot 16): the grid barrier counts arrivals on a counter that is never
+// reset, and launches tag their failure flag with an epoch, so no launch
+// clears anything.
 struct FilterState {
   const void *status = nullptr;  // the buffer the state belongs to ...
   size_t bytes = 0;              // ... and its size (a regrown buffer may reuse the address)
-  uint32_t epoch = 0;            // the last launch's epoch (16-bit tags)
+  uint32_t epoch = 0;            // the last launch's epoch
+  uint64_t arrivals = 0;         // barrier arrivals so far (the counter's value)
   uint32_t grid = 0;             // resident CTAs of the cooperative launch (0: not yet measured)
 };
 
