@@ -638,7 +638,25 @@ def filter_measure(idx, metas, labels, ts, warmup: int, reps: int, batches=(1, 8
         del out, counts
     res["value"] = res["p1"]["value"]
     res["frac"] = res["p1"]["frac"]
-    del flush
+    # context: a device-to-device copy (torch) moving the same bytes as a
+    # one-predicate call (half read, half written), timed the same way
+    nbytes = int(np.mean([8.0 * n + 4.0 * float(c) for c in want[:64]]))
+    src = torch.empty(nbytes // 8, dtype=torch.float32, device="cuda")
+    dst = torch.empty_like(src)
+    cms = []
+    for rep in range(3 + 20):
+        flush.zero_()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        dst.copy_(src)
+        e1.record(stream)
+        e1.synchronize()
+        if rep >= 3:
+            cms.append(e0.elapsed_time(e1))
+    cgbs = 2.0 * src.numel() * 4 / (float(np.median(cms)) * 1e-3) / 1e9
+    res["same_bytes_copy"] = {"value": cgbs, "frac": cgbs / pk, "bytes": int(2 * src.numel() * 4),
+                              "what": "torch device-to-device copy of the same total bytes, L2 flushed, median"}
+    del flush, src, dst
     return res
 
 
