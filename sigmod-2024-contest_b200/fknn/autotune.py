@@ -50,12 +50,12 @@ def table_key(device: str, n: int, mode: int) -> str:
     return f"{device}|n=1e{int(round(np.log10(max(n, 1))))}|mode={mode}"
 
 
-def _timed(index, q, m, mode, kprime, reps):
+def _timed(index, q, m, mode, kprime, reps, graph=False):
     ids = dd = None
     times = []
     for r in range(reps + 1):
         t0 = time.perf_counter()
-        ids, dd = index.search(q, m, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd)
+        ids, dd = index.search(q, m, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, graph=graph)
         if hasattr(ids, "is_cuda"):
             import torch
             torch.cuda.synchronize()
@@ -66,10 +66,13 @@ def _timed(index, q, m, mode, kprime, reps):
 
 
 def autotune(index, qvecs, metas, mode: int, recall_target: float = 0.99, reps: int = 3,
-             kprimes=None, log=None) -> Dict:
+             kprimes=None, log=None, graph: bool = True) -> Dict:
     """Tunes `index` for `mode` on the query sample (qvecs, metas: host or
     torch CUDA arrays).  Leaves the index set to the best setting and
-    returns it: {"tuning": {...}, "kprime": k', "ms": ..., "recall": ...}."""
+    returns it: {"tuning": {...}, "kprime": k', "ms": ..., "recall": ...}.
+    graph: time the reduced-precision modes in their captured form (the
+    plan built on the device), as the bench and serving use them."""
+    graph = graph and mode != _lib.MODE_EXACT_FP32
     exact_ms, gt = _timed(index, qvecs, metas, _lib.MODE_EXACT_FP32, 0, reps)
     space = EXACT_SPACE if mode == _lib.MODE_EXACT_FP32 else SPACE
     cur = index.get_tuning(mode)
@@ -78,7 +81,7 @@ def autotune(index, qvecs, metas, mode: int, recall_target: float = 0.99, reps: 
     def run(tuning, kprime):
         index.set_tuning(mode, tuning["list_slack"], tuning["items_per_sm"], tuning["min_chunk_blocks"],
                          tuning["bound_refresh"], tuning["pilot_stride"])
-        ms, ids = _timed(index, qvecs, metas, mode, kprime, reps)
+        ms, ids = _timed(index, qvecs, metas, mode, kprime, reps, graph)
         rec = 1.0 if mode == _lib.MODE_EXACT_FP32 else recall_matrix(ids, gt)
         if log:
             log(json.dumps({"tuning": tuning, "kprime": kprime, "ms": ms * 1e3, "recall": rec}))
@@ -112,6 +115,7 @@ def autotune(index, qvecs, metas, mode: int, recall_target: float = 0.99, reps: 
                      t["pilot_stride"])
     best["ms"] *= 1e3
     best["exact_ms"] = exact_ms * 1e3
+    best["plan"] = "device, captured graph" if graph else "host"
     return best
 
 
