@@ -188,6 +188,32 @@ def test_filter_rows_batch_matches_oracle(n):
     assert counts_h[17] == 0 and counts_h[20] == n and counts_h[18] >= 1
 
 
+def test_filter_rows_fractional_and_negative_labels():
+    """The label test is int32(label) == int32(v) (utils.h:118): labels that
+    are not integers, negative labels, zero, values truncating from either
+    side, large magnitudes and fractional predicate values; the compaction
+    evaluates it as a float interval, which must select the same rows."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(11)
+    n = 300_001
+    base = np.array([-3.7, -3.0, -2.999, -0.5, -0.0, 0.0, 0.5, 0.999, 1.0, 1.5, 2.0, 2.999999, 3.0, 7.25,
+                     16777216.0, 16777218.0, -16777216.0, 1e9, -1e9, 2147483520.0], np.float32)
+    labels = base[rng.integers(0, len(base), n)]
+    ts = rng.random(n, dtype=np.float32)
+    vecs = np.zeros((n, 100), np.float32)
+    vals = [-4, -3, -2, -1, 0, 1, 2, 3, 7, 16777216, 16777217, 16777218, -16777216, 1000000000, -1000000000,
+            2147483520, 2.5, -2.5, 0.9, -0.9]
+    preds = np.array([[1, v, 0, 0] for v in vals] + [[3, v, 0.2, 0.7] for v in vals[:8]], np.float32)
+    with fknn.Index(vecs, labels, ts) as idx:
+        out, counts = idx.filter_rows_batch(preds)
+        torch.cuda.synchronize()
+        out_h, counts_h = out.cpu().numpy().view(np.uint32), counts.cpu().numpy()
+    for p in range(preds.shape[0]):
+        want = oracle.filter_rows(labels, ts, preds[p])
+        assert counts_h[p] == len(want), (p, preds[p], counts_h[p], len(want))
+        np.testing.assert_array_equal(out_h[p, :len(want)], want)
+
+
 def test_invalid_queries_rejected():
     vecs, labels, ts, q, metas = datagen.make_workload(1, n=5000, nq=4)
     with fknn.Index(vecs, labels, ts) as idx:
