@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstring>
 #include <deque>
+#include <thread>
 #include <vector>
 
 #include "device_util.cuh"
@@ -836,39 +837,57 @@ int fknn_router_search(fknn_router *r, const float *qvecs, const float *metas, u
       }
     if ((rc = run_stage(B, BB, true))) return rc;
     S.ms_type0 = lap();
-    // the pools, in the reference's order of offers (a query meets a bucket once)
-    auto offer_graph = [&](const GBatch &b) {
-      const fknn_router::Sub &sub = subs(b.sub);
-      for (size_t j = 0; j < b.list->size(); ++j) {
-        fknn::IntPool &pl = pool[(*b.list)[j]];
-        if (pl.cap == 0) pl.reset((int)R);
-        const size_t o = b.o0 + j * R;
-        for (uint32_t t = 0; t < R; ++t) pl.offer(h_ids[o + t] + (int)sub.start, (int)h_d[o + t]);
-      }
-    };
-    for (size_t i = 0; i < n0; ++i) offer_graph(B[i]);
+    // the pools, in the reference's order of offers (a query meets a bucket
+    // once); the queries split over host threads, each running the whole
+    // order for its own range of query ids (the lists are ascending)
     const uint32_t kb = P.bf_refine_k;
-    for (size_t k = 0; k < bk_b0.size(); ++k) {
-      for (size_t i = bk_b0[k]; i < bk_b1[k]; ++i) offer_graph(B[i]);
-      if (bk_bb[k] == SIZE_MAX) continue;
-      // SQ8 distances over the bucket's own codes times alpha^2 (:399-417, bruteforce.h:267)
-      const BBatch &b = BB[bk_bb[k]];
-      const fknn_router::Sub &sub = subs(b.sub);
-      const int8_t *bcodes;
-      float ba;
-      uint32_t bn;
-      graph_codes(sub.g, &bcodes, &ba, &bn);
-      for (size_t j = 0; j < b.list.size(); ++j) {
-        fknn::IntPool &pl = pool[b.list[j]];
-        if (pl.cap == 0) pl.reset((int)R);
-        for (uint32_t t = 0; t < kb; ++t) {
-          const uint64_t key = h_keys[b.k0 + j * kb + t];
-          if (key == ~0ull) break;
-          const float dist = (float)(uint32_t)(key >> 32) * ba * ba;
-          pl.offer((int)(sub.start + b.s[j] + (uint32_t)key), (int)dist);
+    auto merge_range = [&](uint32_t lo, uint32_t hi) {
+      auto span = [&](const std::vector<uint32_t> &L, size_t &a, size_t &b) {
+        a = (size_t)(std::lower_bound(L.begin(), L.end(), lo) - L.begin());
+        b = (size_t)(std::lower_bound(L.begin(), L.end(), hi) - L.begin());
+      };
+      auto offer_graph = [&](const GBatch &b) {
+        const fknn_router::Sub &sub = subs(b.sub);
+        size_t a, e;
+        span(*b.list, a, e);
+        for (size_t j = a; j < e; ++j) {
+          fknn::IntPool &pl = pool[(*b.list)[j]];
+          if (pl.cap == 0) pl.reset((int)R);
+          const size_t o = b.o0 + j * R;
+          for (uint32_t t = 0; t < R; ++t) pl.offer(h_ids[o + t] + (int)sub.start, (int)h_d[o + t]);
+        }
+      };
+      for (size_t i2 = 0; i2 < n0; ++i2) offer_graph(B[i2]);
+      for (size_t k = 0; k < bk_b0.size(); ++k) {
+        for (size_t i2 = bk_b0[k]; i2 < bk_b1[k]; ++i2) offer_graph(B[i2]);
+        if (bk_bb[k] == SIZE_MAX) continue;
+        // SQ8 distances over the bucket's own codes times alpha^2 (:399-417, bruteforce.h:267)
+        const BBatch &b = BB[bk_bb[k]];
+        const fknn_router::Sub &sub = subs(b.sub);
+        const int8_t *bcodes;
+        float ba;
+        uint32_t bn;
+        graph_codes(sub.g, &bcodes, &ba, &bn);
+        size_t a, e;
+        span(b.list, a, e);
+        for (size_t j = a; j < e; ++j) {
+          fknn::IntPool &pl = pool[b.list[j]];
+          if (pl.cap == 0) pl.reset((int)R);
+          for (uint32_t t = 0; t < kb; ++t) {
+            const uint64_t key = h_keys[b.k0 + j * kb + t];
+            if (key == ~0ull) break;
+            const float dist = (float)(uint32_t)(key >> 32) * ba * ba;
+            pl.offer((int)(sub.start + b.s[j] + (uint32_t)key), (int)dist);
+          }
         }
       }
-    }
+    };
+    const uint32_t nth = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> th;
+    for (uint32_t t = 1; t < nth; ++t)
+      th.emplace_back(merge_range, (uint32_t)((uint64_t)nq * t / nth), (uint32_t)((uint64_t)nq * (t + 1) / nth));
+    merge_range(0, (uint32_t)((uint64_t)nq / nth));
+    for (std::thread &x : th) x.join();
   }
   S.ms_type2 = lap();
   // global re-rank of the pools (:465-494), ids through the timestamp order
