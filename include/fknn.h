@@ -198,7 +198,10 @@ int fknn_filter_rows(fknn_index *index, const float *meta4, uint32_t *out_ids, u
  * are complete when `stream` reaches the point of the call.  A count of
  * UINT64_MAX means the kernel's bounded wait gave up (its ids are then
  * incomplete); it does not happen in normal operation.  Calls on one index
- * share its scratch: issue them on one stream. */
+ * share its scratch and continue its grid-barrier counter: issue them on
+ * one stream, and do not capture them into a CUDA graph (each launch's
+ * barrier target and epoch are set on the host).  One cooperative launch
+ * per 16 predicates: it starts when all its CTAs (two per SM) fit. */
 int fknn_filter_rows_batch(fknn_index *index, const float *metas, uint32_t np, uint32_t *out_ids,
                            uint64_t *counts, void *stream);
 
