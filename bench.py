@@ -307,13 +307,16 @@ def run_sweep(args):
     def run(mode, kprime):
         ids = torch.empty((nq, 100), dtype=torch.int32, device="cuda")
         dd = torch.empty((nq, 100), dtype=torch.float32, device="cuda")
+        graph = args.plan == "graph" and mode != fknn.MODE_EXACT_FP32
         for _ in range(args.warmup):
-            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream)
+            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream,
+                       graph=graph)
         torch.cuda.synchronize()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(args.steps):
-            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream)
+            idx.search(dq, dm, k=100, mode=mode, kprime=kprime, ids=ids, dists=dd, stream=stream.cuda_stream,
+                       graph=graph)
         e1.record(stream)
         torch.cuda.synchronize()
         return e0.elapsed_time(e1) / args.steps, ids.cpu().numpy().view(np.uint32).copy(), dd.cpu().numpy()
