@@ -7,7 +7,9 @@
  *
  * Pointers passed to fknn_search / fknn_sq8_* may be host memory (pageable
  * or pinned) or device memory on the index's device; the library tells them
- * apart with cudaPointerGetAttributes and copies as needed.
+ * apart with cudaPointerGetAttributes and copies as needed.  Device memory
+ * of another GPU is refused with FKNN_EINVAL by every entry point (the
+ * SQ8 calls compare with the calling thread's current device).
  *
  * Reference interfaces replaced (paths inside KevinZeng08/sigmod-2024-contest):
  *   fknn_bruteforce_rows   <- Bruteforce(nodes, queries, gt)          utils.h:80

@@ -75,15 +75,29 @@ int hs_get(fknn_index *idx, int slot, size_t bytes, void **p) {
   return FKNN_OK;
 }
 
-static bool is_device_ptr(const void *p) {
-  if (!p) return false;
+MemLoc mem_loc(const void *p, int dev) {
+  if (!p) return MemLoc::Host;
   cudaPointerAttributes a;
   if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
     cudaGetLastError();
-    return false;
+    return MemLoc::Host;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  if (a.type == cudaMemoryTypeManaged) return MemLoc::Here;
+  if (a.type == cudaMemoryTypeDevice) return a.device == dev ? MemLoc::Here : MemLoc::Other;
+  return MemLoc::Host;
 }
+
+int check_local_buffers(const char *fn, int dev, std::initializer_list<const void *> bufs) {
+  for (const void *p : bufs)
+    if (p && mem_loc(p, dev) == MemLoc::Other) {
+      set_error(std::string(fn) + ": a buffer is device memory of another device (device " + std::to_string(dev) +
+                " runs this call)");
+      return FKNN_EINVAL;
+    }
+  return FKNN_OK;
+}
+
+static bool is_device_ptr(const void *p, int dev) { return mem_loc(p, dev) == MemLoc::Here; }
 
 static void free_index(fknn_index *idx) {
   if (!idx) return;
@@ -336,8 +350,10 @@ int fknn_search_ex(fknn_index *idx, const float *qvecs, const float *metas, uint
   const float *d_q = qvecs, *d_meta = metas;
   uint32_t *d_ids = ids;
   float *d_dists = dists;
-  const bool q_dev = is_device_ptr(qvecs), m_dev = is_device_ptr(metas);
-  const bool i_dev = is_device_ptr(ids), dd_dev = dists ? is_device_ptr(dists) : true;
+  const int dev = idx->device;
+  if ((rc = check_local_buffers("fknn_search", dev, {qvecs, metas, ids, dists}))) return rc;
+  const bool q_dev = is_device_ptr(qvecs, dev), m_dev = is_device_ptr(metas, dev);
+  const bool i_dev = is_device_ptr(ids, dev), dd_dev = dists ? is_device_ptr(dists, dev) : true;
   if (!q_dev) {
     if ((rc = ws_get(idx, 0, (size_t)nq * DIM * 4, (void **)&d_q))) return rc;
     FKNN_CUDA(cudaMemcpyAsync((void *)d_q, qvecs, (size_t)nq * DIM * 4, cudaMemcpyHostToDevice, st));
@@ -431,7 +447,8 @@ int fknn_count_matches(fknn_index *idx, const float *metas, uint32_t nq, uint32_
   int rc;
   const float *d_meta = metas;
   uint32_t *d_c = counts;
-  const bool m_dev = is_device_ptr(metas), c_dev = is_device_ptr(counts);
+  if ((rc = check_local_buffers("fknn_count_matches", idx->device, {metas, counts}))) return rc;
+  const bool m_dev = is_device_ptr(metas, idx->device), c_dev = is_device_ptr(counts, idx->device);
   if (!m_dev) {
     if ((rc = ws_get(idx, 1, (size_t)nq * 16, (void **)&d_meta))) return rc;
     FKNN_CUDA(cudaMemcpyAsync((void *)d_meta, metas, (size_t)nq * 16, cudaMemcpyHostToDevice, st));
@@ -455,7 +472,8 @@ int fknn_filter_rows(fknn_index *idx, const float *meta4, uint32_t *out_ids, uin
   FKNN_CUDA(cudaSetDevice(idx->device));
   cudaStream_t st = (cudaStream_t)stream;
   uint32_t *d_out = out_ids;
-  const bool o_dev = is_device_ptr(out_ids);
+  if ((rc = check_local_buffers("fknn_filter_rows", idx->device, {out_ids}))) return rc;
+  const bool o_dev = is_device_ptr(out_ids, idx->device);
   if (!o_dev)
     if ((rc = ws_get(idx, 8, (size_t)idx->n * 4, (void **)&d_out))) return rc;
   if ((rc = filter_rows(idx, meta4, d_out, count, st))) return rc;
@@ -477,8 +495,8 @@ int fknn_filter_rows_batch(fknn_index *idx, const float *metas, uint32_t np, uin
   if (np == 0) return FKNN_OK;
   std::lock_guard<std::mutex> lock(idx->mu);
   FKNN_CUDA(cudaSetDevice(idx->device));
-  if (!is_device_ptr(out_ids) || !is_device_ptr(counts)) {
-    set_error("fknn_filter_rows_batch: out_ids and counts must be device memory");
+  if (!is_device_ptr(out_ids, idx->device) || !is_device_ptr(counts, idx->device)) {
+    set_error("fknn_filter_rows_batch: out_ids and counts must be device memory of the index's device");
     return FKNN_EINVAL;
   }
   return filter_rows_batch(idx, metas, np, out_ids, counts, (cudaStream_t)stream);

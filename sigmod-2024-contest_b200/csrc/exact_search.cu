@@ -1324,15 +1324,7 @@ static int noalloc_scratch(uint32_t **out) {
 // True for device memory of device `dev` and for managed memory; false for
 // host memory and for another GPU's memory (its kernels would read a peer's
 // memory, which faults without peer access).
-static bool on_device(const void *p, int dev) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  if (a.type == cudaMemoryTypeManaged) return true;
-  return a.type == cudaMemoryTypeDevice && a.device == dev;
-}
+static bool on_device(const void *p, int dev) { return mem_loc(p, dev) == MemLoc::Here; }
 
 }  // namespace fknn
 

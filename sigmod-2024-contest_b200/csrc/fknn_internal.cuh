@@ -5,6 +5,7 @@
 #include <stdint.h>
 
 #include <functional>
+#include <initializer_list>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -295,6 +296,17 @@ int cuda_fail(cudaError_t e, const char *what);
     cudaError_t _e = (call);                             \
     if (_e != cudaSuccess) return ::fknn::cuda_fail(_e, #call); \
   } while (0)
+
+// Where a caller's buffer lives, for a call that runs on device dev.  This
+// device's memory and managed memory are used in place, host memory is
+// staged through a copy, and another GPU's memory is refused: the kernels
+// here would read or write it as peer memory, which faults without peer
+// access.
+enum class MemLoc { Host, Here, Other };
+MemLoc mem_loc(const void *p, int dev);
+// FKNN_EINVAL (message "<fn>: ... another device") when any non-NULL buffer
+// of bufs is another GPU's memory, else FKNN_OK.
+int check_local_buffers(const char *fn, int dev, std::initializer_list<const void *> bufs);
 
 int dev_alloc(fknn_index *idx, void **p, size_t bytes);
 // index creation around a column builder (capi.cu)

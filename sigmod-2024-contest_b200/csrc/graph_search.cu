@@ -520,14 +520,7 @@ int grow(T **p, size_t *cap, size_t want) {
   return FKNN_OK;
 }
 
-bool on_device(const void *p) {
-  cudaPointerAttributes a;
-  if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
+bool on_device(const void *p, int dev) { return mem_loc(p, dev) == MemLoc::Here; }
 
 void free_graph(fknn_graph *g) {
   if (!g) return;
@@ -861,23 +854,28 @@ int fknn_graph_search(fknn_graph *g, const float *queries, uint32_t nq, int mode
   int32_t *s_ib = reinterpret_cast<int32_t *>(s_b + bf);
   int32_t *s_ids = s_ib + bf;
   float *s_d = reinterpret_cast<float *>(s_ids + of);
+  const int dev = g->device;
+  if ((rc = fknn::check_local_buffers("fknn_graph_search", dev,
+                                      {queries, ranged ? bounds : nullptr, ranged ? id_bounds : nullptr, out_ids,
+                                       out_dists})))
+    return rc;
   const float *q_use = queries;
-  if (!on_device(queries)) {
+  if (!on_device(queries, dev)) {
     FKNN_CUDA(cudaMemcpyAsync(s_q, queries, qf * 4, cudaMemcpyHostToDevice, st));
     q_use = s_q;
   }
   const float *b_use = bounds;
   const int32_t *ib_use = id_bounds;
-  if (ranged && !on_device(bounds)) {
+  if (ranged && !on_device(bounds, dev)) {
     FKNN_CUDA(cudaMemcpyAsync(s_b, bounds, bf * 4, cudaMemcpyHostToDevice, st));
     b_use = s_b;
   }
-  if (ranged && !on_device(id_bounds)) {
+  if (ranged && !on_device(id_bounds, dev)) {
     FKNN_CUDA(cudaMemcpyAsync(s_ib, id_bounds, bf * 4, cudaMemcpyHostToDevice, st));
     ib_use = s_ib;
   }
-  int32_t *ids_use = on_device(out_ids) ? out_ids : s_ids;
-  float *d_use = out_dists ? (on_device(out_dists) ? out_dists : s_d) : nullptr;
+  int32_t *ids_use = on_device(out_ids, dev) ? out_ids : s_ids;
+  float *d_use = out_dists ? (on_device(out_dists, dev) ? out_dists : s_d) : nullptr;
   FKNN_CUDA(cudaMemsetAsync(g->dflag, 0, 4, st));
   if ((rc = fknn::graph_launch(g, q_use, nq, mode, k, cap, refine, b_use, ib_use, ids_use, d_use, st))) return rc;
   if (ids_use != out_ids) FKNN_CUDA(cudaMemcpyAsync(out_ids, ids_use, of * 4, cudaMemcpyDeviceToHost, st));

@@ -60,14 +60,7 @@ __global__ void __launch_bounds__(RK_THREADS)
   }
 }
 
-bool dev_ptr(const void *p) {
-  cudaPointerAttributes a;
-  if (!p || cudaPointerGetAttributes(&a, p) != cudaSuccess) {
-    cudaGetLastError();
-    return false;
-  }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
-}
+bool dev_ptr(const void *p, int dev) { return mem_loc(p, dev) == MemLoc::Here; }
 
 }  // namespace
 
@@ -108,8 +101,10 @@ extern "C" int fknn_rerank(fknn_index *idx, const float *qvecs, uint32_t nq, con
   const uint32_t *d_c = cand;
   uint32_t *d_ids = ids;
   float *d_d = dists;
-  const bool q_dev = dev_ptr(qvecs), c_dev = dev_ptr(cand), i_dev = dev_ptr(ids);
-  const bool dd_dev = dists ? dev_ptr(dists) : true;
+  const int dev = idx->device;
+  if ((rc = check_local_buffers("fknn_rerank", dev, {qvecs, cand, ids, dists}))) return rc;
+  const bool q_dev = dev_ptr(qvecs, dev), c_dev = dev_ptr(cand, dev), i_dev = dev_ptr(ids, dev);
+  const bool dd_dev = dists ? dev_ptr(dists, dev) : true;
   if (!q_dev) {
     if ((rc = ws_get(idx, 0, (size_t)nq * DIM * 4, (void **)&d_q))) return rc;
     FKNN_CUDA(cudaMemcpyAsync((void *)d_q, qvecs, (size_t)nq * DIM * 4, cudaMemcpyHostToDevice, st));

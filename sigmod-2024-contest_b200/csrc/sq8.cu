@@ -523,13 +523,14 @@ __global__ void __launch_bounds__(SQ_WARPS * 32, 4)
   write_heap(heap, k, q, closest, dists, alpha, lane);
 }
 
+// Device memory of the current device (or managed memory).
 bool is_dev(const void *p) {
-  cudaPointerAttributes a;
-  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) {
     cudaGetLastError();
     return false;
   }
-  return a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged;
+  return mem_loc(p, dev) == MemLoc::Here;
 }
 
 struct Scoped {
@@ -579,6 +580,9 @@ int sq8_encode_impl(const float *vecs, uint64_t n, float alpha, int8_t *codes, b
   }
   int rc = ensure_device();
   if (rc) return rc;
+  int dev = 0;
+  FKNN_CUDA(cudaGetDevice(&dev));
+  if ((rc = check_local_buffers("fknn_sq8", dev, {vecs, codes}))) return rc;
   cudaStream_t st = 0;
   Scoped sin, sout, sa;
   const float *d_x;
@@ -677,6 +681,7 @@ int sq8_bf_impl(size_t k, int *closest, float *dists, size_t npoints, const char
   if (rc) return rc;
   int dev = 0;
   FKNN_CUDA(cudaGetDevice(&dev));
+  if ((rc = check_local_buffers("fknn_sq8_bruteforce", dev, {closest, dists, codes_in, queries_in}))) return rc;
   Sq8Scratch &scr = sq8_scratch();
   if (scr.device != dev) {
     // once per thread and device: stream, event, SM count, and the kernels'
