@@ -623,6 +623,13 @@ __global__ void __launch_bounds__(B_THREADS, 2)
       Candidate *list = out + ((uint64_t)item_id * BQ + L) * capb;
       int cnt = 0;
       bool ok = !aborted;
+      // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc);
+      // with no bound yet every column of the slab is one (cq = -FLT_MAX),
+      // and columns outside the slab are -inf, which no cq admits.  cq is
+      // recomputed only when T changes.
+      auto acc_bound = [&](float t) { return (t == INFINITY) ? -FLT_MAX : 0.5f * (qn - t) / sc; };
+      float cq = acc_bound(T);
+      uint32_t until_refresh = refresh;  // sub-tiles until the next read of the shared bound
       for (uint32_t sub = 0; sub < nsub && ok; ++sub) {
         const uint32_t gs = g + sub;
         const int ab = gs & 1;
@@ -635,10 +642,6 @@ __global__ void __launch_bounds__(B_THREADS, 2)
         const uint32_t p0 = (it.blk0 + sub * stride) * BR;
         const int r0 = (int)min(max(s, p0), p0 + BR) - (int)p0;
         const int r1 = (int)min(max(e, p0), p0 + BR) - (int)p0;
-        // candidate iff qn - 2*sc*acc <= T  <=>  acc >= (qn - T) / (2 sc);
-        // with no bound yet every column of the slab is one (cq = -FLT_MAX),
-        // and columns outside the slab are -inf, which no cq admits
-        const float cq = (T == INFINITY) ? -FLT_MAX : 0.5f * (qn - T) / sc;
         // four 32-column chunks; the TMEM load of the next chunk is in flight
         // while this one is screened
         const uint32_t tb = tmem + ((uint32_t)(wg * 32) << 16) + ab * BR;
@@ -675,13 +678,19 @@ __global__ void __launch_bounds__(B_THREADS, 2)
           }
           cnt = sm.cnt[L];
           T = sm.thr[L];
+          cq = acc_bound(T);
         }
         // other items of the same query tighten the shared bound meanwhile
-        if (refresh && sub % refresh == refresh - 1 && qi >= 0) {
-          const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
-          if (Tg < T) {
-            T = Tg;
-            sm.thr[L] = T;
+        // (every refresh-th sub-tile of the item)
+        if (refresh && --until_refresh == 0) {
+          until_refresh = refresh;
+          if (qi >= 0) {
+            const float Tg = sortable_f32(ld_volatile_u32(T_global + qi));
+            if (Tg < T) {
+              T = Tg;
+              sm.thr[L] = T;
+              cq = acc_bound(T);
+            }
           }
         }
       }
